@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 semi-local LCS engine.
+
+Metric: GCUPS (cell updates per second / 1e9) of the batched, tuned combing
+path on the read-versus-window workload (20,000 pairs, lognormal read lengths),
+with the plain per-pair launch loop and the 2^20 x 2^20 pair measured beside
+it, and the dominant kernel stated against the measured integer roofline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl slcs|reference]
+
+Under torchrun (N > 1) every rank combs its own batch (weak scaling, no
+data-path collective); the time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "platform-independent-lcs_b200"))
+
+METRIC = "GCUPS on 1 B200: batched+cost-model-tuned vs plain per-pair; % of INT roofline"
+UNIT = "GCUPS"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["slcs", "reference"], default="slcs")
+    ap.add_argument("--no-extras", action="store_true", help="skip the per-pair loop and the 2^20 pair")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region (NVML, read only)
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, device_index: int):
+        self.samples, self.reasons = [], set()
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+        self._stop = threading.Event()
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for b, name in self.REASONS.items():
+                    if bits & b and b != 0x1:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def read_traffic(kernel_key: str):
+    """DRAM bytes per launch recorded from an ncu capture (profiles/*.md)."""
+    prof = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(prof):
+        return None
+    for fn in sorted(os.listdir(prof)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(prof, fn)):
+            if line.startswith(f"traffic_bytes_per_launch[{kernel_key}]:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CPU code (oracle/_ref) on host cores
+# ---------------------------------------------------------------------------
+def run_reference(args, batch):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    kind = "reference"
+    if O.ref_lib() is None:
+        kind = "port"
+    threads = os.cpu_count() or 1
+    sample = min(batch.npairs, 4000)
+    ms = batch.ms[:sample]
+    ns = batch.ns[:sample]
+    cells = int(np.sum(ms.astype(np.int64) * ns))
+    sizes = ms.astype(np.int64) + ns
+    off = np.zeros(sample, np.int64)
+    off[1:] = np.cumsum(sizes)[:-1]
+    total = int(sizes.sum())
+    if kind == "reference":
+        ab, bb = batch.a_blob.astype(np.int32), batch.b_blob.astype(np.int32)
+        step = lambda: O.ref_comb_batch(ab, bb, batch.a_off[:sample], batch.b_off[:sample], ms, ns, off, total,
+                                        nthreads=threads)
+    else:
+        step = lambda: O.comb_batch(batch.a_blob, batch.b_blob, batch.a_off[:sample], batch.b_off[:sample], ms, ns,
+                                    off, total, nthreads=threads)
+    for _ in range(max(1, min(args.warmup, 2))):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    value = cells / dt / 1e9
+    desc = f"first {sample} of the {batch.npairs} read/window pairs ({cells} cells) per step"
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "reads_20000", "pairs": batch.npairs, "sample_pairs": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def cpu_baseline(batch):
+    """The reference's CPU code timed on this host's cores on the whole batch."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads = os.cpu_count() or 1
+    off, total = batch.strand_offsets()
+    if O.ref_lib() is not None:
+        ab, bb = batch.a_blob.astype(np.int32), batch.b_blob.astype(np.int32)
+        t0 = time.perf_counter()
+        out = O.ref_comb_batch(ab, bb, batch.a_off, batch.b_off, batch.ms, batch.ns, off, total, nthreads=threads)
+        dt = time.perf_counter() - t0
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        out = O.comb_batch(batch.a_blob, batch.b_blob, batch.a_off, batch.b_off, batch.ms, batch.ns, off, total,
+                           nthreads=threads)
+        dt = time.perf_counter() - t0
+        kind = "port"
+    return {"value": batch.cells / dt / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"all {batch.npairs} pairs ({batch.cells} cells), one pass, {dt:.2f} s"}, out
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    from slcs import workloads as W
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        batch = W.reads_20000()
+        print(json.dumps(run_reference(args, batch)), flush=True)
+        return 0
+
+    import torch
+    import slcs
+    from slcs import tuning
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+
+    batch = W.reads_20000(seed=4 + rank)
+    descs = slcs.pair_descs(batch)
+    _, total = batch.strand_offsets()
+    cfg, tuned_by = tuning.choose_batch_config(batch)
+    plan = slcs.BatchPlan(descs, cfg)
+    a_d = torch.from_numpy(batch.a_blob).to(dev)
+    b_d = torch.from_numpy(batch.b_blob).to(dev)
+    out = torch.empty(total, dtype=torch.int32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    int_ops, cell_rate = slcs.probe_int_rates()
+    roof_gcups = int_ops / 5.0 / 1e9
+
+    for _ in range(args.warmup):
+        plan.run(a_d, b_d, out)
+        flush.zero_()
+    torch.cuda.synchronize()
+    slcs.device_status(local)
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with sampler:
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record(stream)
+            plan.run(a_d, b_d, out)
+            e1.record(stream)
+        torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    slcs.device_status(local)
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    total_ms = float(sum(step_ms))
+    if pg:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    cells_all = batch.cells * world
+    value = cells_all / (ms_per_step * 1e-3) / 1e9
+    kern_gcups = batch.cells / (ms_per_step * 1e-3) / 1e9
+
+    # parity of the timed output with the committed golden digest (rank 0's batch)
+    bitexact = None
+    if rank == 0:
+        import hashlib
+        g = json.load(open(os.path.join(ROOT, "tests", "golden", "golden.json")))
+        bitexact = hashlib.sha256(out.cpu().numpy().tobytes()).hexdigest() == g["reads_20000"]["sha256_strands"]
+
+    # end to end: host buffers through the C ABI, copies inside the timed region
+    a_h = torch.from_numpy(batch.a_blob).pin_memory().numpy()
+    b_h = torch.from_numpy(batch.b_blob).pin_memory().numpy()
+    o_h = torch.empty(total, dtype=torch.int32).pin_memory().numpy()
+    for _ in range(2):
+        plan.run_host(a_h, b_h, o_h)
+    if pg:
+        pg.barrier()
+    e2e_steps = max(3, min(args.steps, 50))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        plan.run_host(a_h, b_h, o_h)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if pg:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": cells_all / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(a_h.nbytes + b_h.nbytes),
+           "d2h_bytes_per_step": int(o_h.nbytes), "ms_per_step": e2e_s * 1e3}
+
+    extras = {}
+    if not args.no_extras and rank == 0:
+        extras = tuning.secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "reads_20000", "pairs_per_gpu": batch.npairs, "cells_per_gpu_step": batch.cells,
+                   "variant": {"tile_m": plan_tile_m(cfg), "warps": cfg.warps or 4, "graph": bool(cfg.use_graph)},
+                   "tuned_by": tuned_by, "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"{world} independent batches (weak)"},
+        "e2e": e2e,
+        "gpu_launches": args.steps * plan.launches,
+        "roofline": {"bound": "int32", "achieved": kern_gcups, "peak": roof_gcups, "unit": "GCUPS",
+                     "frac": kern_gcups / roof_gcups, "traffic": read_traffic("reads_20000"),
+                     "peak_source": "measured here: INT32 min/max issue rate / 5 ops per cell",
+                     "int32_tops": int_ops / 1e12, "cell_rule_ceiling_gcups": cell_rate / 1e9},
+        "clocks": sampler.summary(),
+        "bitexact_vs_reference": bitexact,
+    }
+    line.update(extras)
+    if rank == 0 and world == 1:
+        cb, ref_out = cpu_baseline(batch)
+        line["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del plan
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def plan_tile_m(cfg):
+    return cfg.tile_m or 8
+
+
+if __name__ == "__main__":
+    sys.exit(main())

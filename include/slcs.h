@@ -1,0 +1,171 @@
+/*
+ * slcs.h -- C ABI of the B200 semi-local LCS engine (libslcs.so).
+ *
+ * Semi-local LCS by seaweed (strand) combing: for strings a (length m) and
+ * b (length n) the engine returns the strand ids leaving the alignment grid,
+ * h[m] on the right edge and v[n] on the bottom edge, exactly as the
+ * reference's CPU procedure Lcs_Semi_Reference2 produces them
+ * (src/lcs_residual_fixup.hpp:4-70 of egor-bv/platform-independent-lcs), and
+ * the permutation matrix built from them (src/permutation_matrix.hpp:88-115).
+ *
+ * Conventions
+ *   - Symbols are bytes; only equality matters (the reference compares Word
+ *     values for equality only, src/lcs_residual_fixup.hpp:50), so any
+ *     injective map of an alphabet of at most 256 symbols onto bytes keeps the
+ *     output bit-exact.
+ *   - Strand ids are int32: h starts as i = m-1-r for row r of a, v starts as
+ *     m+j for column j of b.
+ *   - Functions ending in _host take host pointers and return when the result
+ *     is in host memory.  All others take device pointers and are enqueued on
+ *     `stream` (a cudaStream_t, NULL = legacy default stream); errors raised on
+ *     the device are reported by slcs_device_status().
+ *   - No function throws or aborts.  Each returns an slcs_status; the text of
+ *     the last error of the calling thread is available from slcs_last_error().
+ */
+#ifndef SLCS_H
+#define SLCS_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SLCS_API __attribute__((visibility("default")))
+#else
+#define SLCS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SLCS_OK = 0,
+    SLCS_ERR_INVALID = 1,     /* bad argument (null pointer, negative size, ...)     */
+    SLCS_ERR_ALLOC = 2,       /* device or host allocation failed                   */
+    SLCS_ERR_DEVICE = 3,      /* a CUDA call failed                                 */
+    SLCS_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up                 */
+    SLCS_ERR_UNSUPPORTED = 5, /* configuration not available in this build          */
+    SLCS_ERR_RANGE = 6        /* size beyond a documented limit                     */
+} slcs_status;
+
+/* Kernel family used for combing. */
+enum {
+    SLCS_ALGO_AUTO = 0,      /* let the engine choose (cost model, else heuristic)     */
+    SLCS_ALGO_WAVEFRONT = 1, /* row stripes on warps, strands handed down through HBM */
+    SLCS_ALGO_STRIPS = 2     /* column strips combed independently, then braid-merged */
+};
+
+/* Tuning knobs.  Zero in any field means "engine default". */
+typedef struct {
+    int32_t algo;          /* SLCS_ALGO_*                                            */
+    int32_t tile_m;        /* rows of a held in registers by one lane (2..16)         */
+    int32_t tile_n;        /* columns combed per wavefront step (4)                   */
+    int32_t warps;         /* warps per thread block                                  */
+    int32_t braid_cutoff;  /* steady-ant size below which one block finishes a node   */
+    int32_t strips;        /* column strips for SLCS_ALGO_STRIPS                      */
+    int32_t use_graph;     /* batch plans: replay the launch as a captured CUDA graph */
+    int32_t reserved[9];
+} slcs_config;
+
+/* One pair of a batch: symbols at a_blob[a_offset .. +m) and b_blob[b_offset .. +n);
+ * its strands are written to out[out_offset .. +m) (h) then [.. +m+n) (v). */
+typedef struct {
+    int64_t a_offset;
+    int64_t b_offset;
+    int64_t out_offset;
+    int32_t m;
+    int32_t n;
+} slcs_pair_desc;
+
+typedef struct slcs_batch_plan slcs_batch_plan;
+
+/* ---- errors ------------------------------------------------------------ */
+SLCS_API const char *slcs_last_error(void);
+SLCS_API const char *slcs_status_string(slcs_status s);
+/* Error bits raised by kernels on `device` since the last clear (0 = none).
+ * Synchronise the stream first.  Replaces the reference's exception path
+ * (src/main.cpp:83-94). */
+SLCS_API slcs_status slcs_device_status(int32_t device, int32_t clear);
+SLCS_API void slcs_default_config(slcs_config *cfg);
+SLCS_API int32_t slcs_version(void);
+/* Make `device` current for the calling thread (the queue the reference's
+ * registry binds per device type, src/algorithm_registry.cpp:6-41). */
+SLCS_API slcs_status slcs_set_device(int32_t device);
+/* Name of `device` (for the CSV "device" column, src/main.cpp:70). */
+SLCS_API slcs_status slcs_device_name(int32_t device, char *buf, int32_t len);
+
+/* ---- combing ----------------------------------------------------------- */
+
+/* One pair, device pointers.  Replaces the LcsProcedure call
+ * (src/lcs_interface_internal.hpp:91) of Lcs_Semi_Reference2 /
+ * Lcs_Semi_Tiled_* (src/lcs_tiled.hpp:10-251) including the host residual
+ * fixup (src/lcs_grid.hpp:451-493): every cell is combed on the device. */
+SLCS_API slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n,
+                           int32_t *h_out, int32_t *v_out, const slcs_config *cfg, void *stream);
+
+/* One pair, host pointers (copies in, combs, copies out, synchronises).  The
+ * entry point a SemiLocalLcsImpl adapter (src/algorithm_registry.cpp:59-73)
+ * binds. */
+SLCS_API slcs_status slcs_comb_pair_host(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n,
+                                int32_t *h_out, int32_t *v_out, const slcs_config *cfg);
+
+/* Many independent pairs in one persistent launch with a device work queue.
+ * pairs: host array of npairs descriptors; blobs/out: device pointers.
+ * The reference has no batched entry; it would loop over
+ * SemiLocalLcsImpl::operator() (src/main.cpp:58-66). */
+SLCS_API slcs_status slcs_comb_batch(const slcs_pair_desc *pairs, int32_t npairs, const uint8_t *a_blob,
+                            const uint8_t *b_blob, int32_t *out, const slcs_config *cfg, void *stream);
+
+/* Same, host pointers for blobs and output (a_len/b_len/out_len in elements). */
+SLCS_API slcs_status slcs_comb_batch_host(const slcs_pair_desc *pairs, int32_t npairs, const uint8_t *a_blob,
+                                 int64_t a_len, const uint8_t *b_blob, int64_t b_len, int32_t *out,
+                                 int64_t out_len, const slcs_config *cfg);
+
+/* Reusable batch plan: the descriptors, the schedule and the chosen kernel
+ * variant are uploaded once; slcs_batch_plan_run only launches (and, with
+ * cfg->use_graph, replays a captured CUDA graph). */
+SLCS_API slcs_status slcs_batch_plan_create(slcs_batch_plan **plan, const slcs_pair_desc *pairs, int32_t npairs,
+                                   const slcs_config *cfg);
+SLCS_API slcs_status slcs_batch_plan_run(slcs_batch_plan *plan, const uint8_t *a_blob, const uint8_t *b_blob,
+                                int32_t *out, void *stream);
+/* Host-pointer run of a plan: copies the blobs in on `stream`, runs, copies
+ * the strands out and synchronises (the end-to-end path a host caller uses). */
+SLCS_API slcs_status slcs_batch_plan_run_host(slcs_batch_plan *plan, const uint8_t *a_blob, int64_t a_len,
+                                              const uint8_t *b_blob, int64_t b_len, int32_t *out, int64_t out_len,
+                                              void *stream);
+SLCS_API slcs_status slcs_batch_plan_destroy(slcs_batch_plan *plan);
+/* Kernel launches one slcs_batch_plan_run issues (for launch accounting). */
+SLCS_API int32_t slcs_batch_plan_launches(const slcs_batch_plan *plan);
+
+/* ---- permutation matrix ------------------------------------------------ */
+
+/* PermutationMatrix::FromStrands (src/permutation_matrix.hpp:88-115) on the
+ * device: row_to_col / col_to_row of size m+n (either may be NULL). */
+SLCS_API slcs_status slcs_strands_to_permutation(const int32_t *h, int32_t m, const int32_t *v, int32_t n,
+                                        int32_t *row_to_col, int32_t *col_to_row, void *stream);
+
+/* PermutationMatrix::hash (src/permutation_matrix.hpp:192-203) of a host
+ * col_to_row array, with the reference's signed 64-bit wrap-around. */
+SLCS_API int64_t slcs_permutation_hash(const int32_t *col_to_row, int32_t size);
+
+/* ---- braid multiplication ---------------------------------------------- */
+
+/* staggered_multiply<RowGlue> (src/braid_multiplication.hpp:273-407) of two
+ * full permutations given as device row->col arrays; out_row_to_col receives
+ * p_size + q_size - k entries.  Steady-ant recursion (204-270) runs on the
+ * device; nodes at or below cfg->braid_cutoff are finished by one block. */
+SLCS_API slcs_status slcs_braid_multiply(const int32_t *p_row_to_col, int32_t p_size, const int32_t *q_row_to_col,
+                                int32_t q_size, int32_t k, int32_t row_glue, int32_t *out_row_to_col,
+                                const slcs_config *cfg, void *stream);
+
+/* ---- diagnostics (no counterpart in the reference) --------------------- */
+
+/* Measured integer ceilings of the current device, the denominators of the
+ * combing roofline: the INT32 min/max issue rate (ops/s) and the cell rate
+ * of the combing rule on register-resident strands (cells/s). */
+SLCS_API slcs_status slcs_probe_int_rates(int32_t iters, double *int32_ops_per_s, double *cells_per_s,
+                                          void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SLCS_H */

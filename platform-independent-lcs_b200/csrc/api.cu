@@ -1,0 +1,583 @@
+// api.cu -- the C ABI of libslcs (declared in include/slcs.h).
+//
+// Host logic only: argument checks, schedules (task lists), scratch and
+// workspace management, batch plans with optional CUDA-graph replay, and the
+// synchronous host-pointer wrappers.  All combing runs in comb.cu.
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "comb.cuh"
+
+namespace slcs {
+
+namespace {
+thread_local std::string g_last_error;
+
+struct DeviceState {
+    uint32_t *host_status = nullptr;
+    uint32_t *dev_status = nullptr;
+    int sms = 0;
+    bool init = false;
+};
+std::mutex g_dev_mu;
+DeviceState g_dev[64];
+
+DeviceState &dev_state()
+{
+    int d = 0;
+    cudaGetDevice(&d);
+    if (d < 0 || d >= 64) d = 0;
+    std::lock_guard<std::mutex> g(g_dev_mu);
+    DeviceState &s = g_dev[d];
+    if (!s.init) {
+        s.init = true;
+        cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, d);
+        if (s.sms <= 0) s.sms = 148;
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, 64, cudaHostAllocMapped) == cudaSuccess) {
+            s.host_status = static_cast<uint32_t *>(p);
+            *s.host_status = 0;
+            void *dp = nullptr;
+            if (cudaHostGetDevicePointer(&dp, p, 0) == cudaSuccess) s.dev_status = static_cast<uint32_t *>(dp);
+        } else {
+            cudaGetLastError();
+        }
+    }
+    return s;
+}
+
+int pick_tile_m(const slcs_config *cfg, int32_t m_typical, int64_t total_cells)
+{
+    if (cfg && cfg->tile_m) return cfg->tile_m;
+    (void)total_cells;
+    if (m_typical >= 65536) return 8;
+    if (m_typical >= 8192) return 4;
+    if (m_typical <= 64) return 2;
+    if (m_typical <= 128) return 4;
+    return 8;
+}
+
+int pick_warps(const slcs_config *cfg) { return (cfg && cfg->warps) ? cfg->warps : 4; }
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+__global__ void identity_strands_kernel(int32_t *h, int32_t m, int32_t *v, int32_t n)
+{
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m + n; i += gridDim.x * blockDim.x) {
+        if (i < m) h[i] = i;
+        else v[i - m] = i;
+    }
+}
+
+// Host schedule of a batch: pairs ordered by cells (largest first), each
+// pair's stripes as consecutive tasks, scratch rows for multi-stripe pairs.
+struct Schedule {
+    std::vector<int2> tasks;
+    std::vector<int64_t> scratch_off;
+    int64_t scratch_elems = 0;
+};
+
+Schedule build_schedule(const slcs_pair_desc *pairs, int32_t npairs, int tm)
+{
+    Schedule S;
+    std::vector<int32_t> order(npairs);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+        return int64_t(pairs[x].m) * pairs[x].n > int64_t(pairs[y].m) * pairs[y].n;
+    });
+    S.scratch_off.assign(npairs, 0);
+    for (int32_t p : order) {
+        const int32_t st = (pairs[p].n > 0) ? stripes_of(pairs[p].m, tm) : 0;
+        for (int32_t s = 0; s < st; ++s) S.tasks.push_back(make_int2(p, s));
+        const int64_t e = scratch_elems(pairs[p].m, pairs[p].n, tm);
+        if (e) {
+            S.scratch_off[p] = S.scratch_elems;
+            S.scratch_elems += e;
+        }
+    }
+    return S;
+}
+
+slcs_status check_pairs(const slcs_pair_desc *pairs, int32_t npairs)
+{
+    if (npairs < 0) return fail(SLCS_ERR_INVALID, "npairs must be >= 0");
+    if (npairs > 0 && !pairs) return fail(SLCS_ERR_INVALID, "pairs is null");
+    for (int32_t p = 0; p < npairs; ++p) {
+        const slcs_pair_desc &d = pairs[p];
+        if (d.m < 0 || d.n < 0 || d.a_offset < 0 || d.b_offset < 0 || d.out_offset < 0)
+            return fail(SLCS_ERR_INVALID, "pair " + std::to_string(p) + ": negative size or offset");
+        if (int64_t(d.m) + d.n > INT32_MAX)
+            return fail(SLCS_ERR_RANGE, "pair " + std::to_string(p) + ": m+n exceeds int32 strand ids");
+    }
+    return SLCS_OK;
+}
+
+} // namespace
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+slcs_status fail(slcs_status s, const std::string &msg)
+{
+    g_last_error = msg;
+    return s;
+}
+slcs_status cuda_fail(cudaError_t e, const char *what)
+{
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return SLCS_ERR_DEVICE;
+}
+uint32_t *device_status_word() { return dev_state().dev_status; }
+int sm_count() { return dev_state().sms; }
+
+// Pairs with an empty side have no cells: the strands keep their start ids.
+static slcs_status write_identity(int32_t *h, int32_t m, int32_t *v, int32_t n, cudaStream_t st)
+{
+    if (m + n == 0) return SLCS_OK;
+    identity_strands_kernel<<<(m + n + 255) / 256 < 1024 ? (m + n + 255) / 256 : 1024, 256, 0, st>>>(h, m, v, n);
+    SLCS_CUDA(cudaGetLastError());
+    return SLCS_OK;
+}
+
+} // namespace slcs
+
+using namespace slcs;
+
+struct slcs_batch_plan {
+    int device = 0;
+    int tm = 8;
+    int warps = 4;
+    int32_t npairs = 0;
+    int32_t ntasks = 0;
+    bool use_graph = false;
+    PairDev *d_pairs = nullptr;
+    int2 *d_tasks = nullptr;
+    int64_t *d_scr_off = nullptr;
+    int32_t *d_scratch = nullptr;
+    int32_t *d_work = nullptr; // [counters(4) | progress(ntasks)]
+    size_t work_bytes = 0;
+    std::vector<slcs_pair_desc> empty_pairs; // pairs with m == 0 or n == 0
+    cudaGraphExec_t gexec = nullptr;
+    const void *g_a = nullptr, *g_b = nullptr, *g_out = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    // Extents the descriptors reach (elements), checked by the host-pointer run.
+    int64_t need_a = 0, need_b = 0, need_out = 0;
+    // Device staging of slcs_batch_plan_run_host, grown on demand.
+    char *h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+
+    CombLaunch launch(const uint8_t *a, const uint8_t *b, int32_t *out) const
+    {
+        CombLaunch L{};
+        L.pairs = d_pairs;
+        L.tasks = d_tasks;
+        L.ntasks = ntasks;
+        L.a_blob = a;
+        L.b_blob = b;
+        L.out = out;
+        L.scratch = d_scratch;
+        L.scratch_off = d_scr_off;
+        L.counters = d_work;
+        L.progress = d_work + 4;
+        L.status = device_status_word();
+        return L;
+    }
+
+    slcs_status enqueue(const uint8_t *a, const uint8_t *b, int32_t *out, cudaStream_t st) const
+    {
+        SLCS_CUDA(cudaMemsetAsync(d_work, 0, work_bytes, st));
+        slcs_status s = launch_comb(launch(a, b, out), tm, warps, st, nullptr);
+        if (s != SLCS_OK) return s;
+        for (const auto &d : empty_pairs) {
+            s = write_identity(out + d.out_offset, d.m, out + d.out_offset + d.m, d.n, st);
+            if (s != SLCS_OK) return s;
+        }
+        return SLCS_OK;
+    }
+};
+
+extern "C" {
+
+const char *slcs_last_error(void) { return g_last_error.c_str(); }
+
+const char *slcs_status_string(slcs_status s)
+{
+    switch (s) {
+    case SLCS_OK: return "ok";
+    case SLCS_ERR_INVALID: return "invalid argument";
+    case SLCS_ERR_ALLOC: return "allocation failed";
+    case SLCS_ERR_DEVICE: return "CUDA error";
+    case SLCS_ERR_TIMEOUT: return "device wait timed out";
+    case SLCS_ERR_UNSUPPORTED: return "unsupported configuration";
+    case SLCS_ERR_RANGE: return "size out of range";
+    }
+    return "unknown status";
+}
+
+int32_t slcs_version(void) { return 1; }
+
+slcs_status slcs_set_device(int32_t device)
+{
+    SLCS_CUDA(cudaSetDevice(device));
+    return SLCS_OK;
+}
+
+slcs_status slcs_device_name(int32_t device, char *buf, int32_t len)
+{
+    if (!buf || len <= 0) return fail(SLCS_ERR_INVALID, "null buffer");
+    cudaDeviceProp prop;
+    SLCS_CUDA(cudaGetDeviceProperties(&prop, device));
+    std::strncpy(buf, prop.name, size_t(len) - 1);
+    buf[len - 1] = '\0';
+    return SLCS_OK;
+}
+
+void slcs_default_config(slcs_config *cfg)
+{
+    if (cfg) std::memset(cfg, 0, sizeof(*cfg));
+}
+
+slcs_status slcs_device_status(int32_t device, int32_t clear)
+{
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (device != cur) SLCS_CUDA(cudaSetDevice(device));
+    DeviceState &s = dev_state();
+    uint32_t bits = s.host_status ? __atomic_load_n(s.host_status, __ATOMIC_SEQ_CST) : 0;
+    if (clear && s.host_status) __atomic_store_n(s.host_status, 0u, __ATOMIC_SEQ_CST);
+    if (device != cur) cudaSetDevice(cur);
+    if (bits & DEV_ERR_TIMEOUT) return fail(SLCS_ERR_TIMEOUT, "a device-side wait timed out");
+    if (bits) return fail(SLCS_ERR_DEVICE, "device status bits " + std::to_string(bits));
+    return SLCS_OK;
+}
+
+slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n, int32_t *h_out,
+                           int32_t *v_out, const slcs_config *cfg, void *stream)
+{
+    if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
+    if ((m > 0 && (!a || !h_out)) || (n > 0 && (!b || !v_out)))
+        return fail(SLCS_ERR_INVALID, "null pointer for a non-empty side");
+    if (int64_t(m) + n > INT32_MAX) return fail(SLCS_ERR_RANGE, "m+n exceeds int32 strand ids");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (m == 0 || n == 0) return write_identity(h_out, m, v_out, n, st);
+    const int tm = pick_tile_m(cfg, m, int64_t(m) * n);
+    if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+    const int32_t ntasks = stripes_of(m, tm);
+    const size_t work_bytes = align_up(sizeof(int32_t) * (4 + size_t(ntasks)), 256);
+    const size_t scr_bytes = sizeof(int32_t) * size_t(scratch_elems(m, n, tm));
+    void *ws = nullptr;
+    SLCS_CUDA(cudaMallocAsync(&ws, work_bytes + scr_bytes + 16, st));
+    int32_t *work = static_cast<int32_t *>(ws);
+    SLCS_CUDA(cudaMemsetAsync(work, 0, work_bytes, st));
+    CombLaunch L{};
+    L.pairs = nullptr;
+    L.tasks = nullptr;
+    L.ntasks = ntasks;
+    L.a_blob = a;
+    L.b_blob = b;
+    L.out = h_out;
+    L.scratch = reinterpret_cast<int32_t *>(static_cast<char *>(ws) + work_bytes);
+    L.scratch_off = nullptr;
+    L.counters = work;
+    L.progress = work + 4;
+    L.status = device_status_word();
+    L.single.a_off = 0;
+    L.single.b_off = 0;
+    L.single.m = m;
+    L.single.n = n;
+    // h and v may live in separate allocations: address v relative to h.
+    L.single.out_off = 0;
+    slcs_status s;
+    if (v_out == h_out + m) {
+        s = launch_comb(L, tm, pick_warps(cfg), st, nullptr);
+    } else {
+        // Comb into a contiguous temporary, then copy v out.
+        int32_t *tmp = nullptr;
+        SLCS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&tmp), sizeof(int32_t) * (size_t(m) + n), st));
+        L.out = tmp;
+        s = launch_comb(L, tm, pick_warps(cfg), st, nullptr);
+        if (s == SLCS_OK) {
+            SLCS_CUDA(cudaMemcpyAsync(h_out, tmp, sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, st));
+            SLCS_CUDA(cudaMemcpyAsync(v_out, tmp + m, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
+        }
+        SLCS_CUDA(cudaFreeAsync(tmp, st));
+    }
+    SLCS_CUDA(cudaFreeAsync(ws, st));
+    return s;
+}
+
+slcs_status slcs_comb_pair_host(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n, int32_t *h_out,
+                                int32_t *v_out, const slcs_config *cfg)
+{
+    if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
+    if ((m > 0 && (!a || !h_out)) || (n > 0 && (!b || !v_out)))
+        return fail(SLCS_ERR_INVALID, "null pointer for a non-empty side");
+    cudaStream_t st = nullptr;
+    SLCS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const size_t ab = align_up(size_t(m) + 16, 256), bb = align_up(size_t(n) + 16, 256);
+    const size_t sb = sizeof(int32_t) * (size_t(m) + n + 4);
+    char *buf = nullptr;
+    slcs_status s = SLCS_OK;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&buf), ab + bb + sb, st);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(st);
+        return cuda_fail(e, "cudaMallocAsync");
+    }
+    uint8_t *da = reinterpret_cast<uint8_t *>(buf);
+    uint8_t *db = reinterpret_cast<uint8_t *>(buf + ab);
+    int32_t *dout = reinterpret_cast<int32_t *>(buf + ab + bb);
+    if (m) e = cudaMemcpyAsync(da, a, m, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && n) e = cudaMemcpyAsync(db, b, n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        s = slcs_comb_pair(da, m, db, n, dout, dout + m, cfg, st);
+        if (s == SLCS_OK && m) e = cudaMemcpyAsync(h_out, dout, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, st);
+        if (s == SLCS_OK && e == cudaSuccess && n)
+            e = cudaMemcpyAsync(v_out, dout + m, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st);
+    }
+    cudaFreeAsync(buf, st);
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (s != SLCS_OK) return s;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamSynchronize");
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return slcs_device_status(dev, 1);
+}
+
+slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_desc *pairs, int32_t npairs,
+                                   const slcs_config *cfg)
+{
+    if (!plan_out) return fail(SLCS_ERR_INVALID, "plan is null");
+    *plan_out = nullptr;
+    slcs_status s = check_pairs(pairs, npairs);
+    if (s != SLCS_OK) return s;
+    auto *P = new (std::nothrow) slcs_batch_plan();
+    if (!P) return fail(SLCS_ERR_ALLOC, "plan allocation");
+    cudaGetDevice(&P->device);
+    // Typical m: the median of the batch.
+    std::vector<int32_t> ms;
+    ms.reserve(npairs);
+    int64_t cells = 0;
+    for (int32_t p = 0; p < npairs; ++p) {
+        ms.push_back(pairs[p].m);
+        cells += int64_t(pairs[p].m) * pairs[p].n;
+    }
+    int32_t med = 0;
+    if (!ms.empty()) {
+        std::nth_element(ms.begin(), ms.begin() + ms.size() / 2, ms.end());
+        med = ms[ms.size() / 2];
+    }
+    P->tm = pick_tile_m(cfg, med, cells);
+    P->warps = pick_warps(cfg);
+    P->use_graph = cfg && cfg->use_graph;
+    P->npairs = npairs;
+    if (!tile_m_supported(P->tm)) {
+        delete P;
+        return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+    }
+    for (int32_t p = 0; p < npairs; ++p) {
+        if (pairs[p].m == 0 || pairs[p].n == 0) P->empty_pairs.push_back(pairs[p]);
+        P->need_a = std::max<int64_t>(P->need_a, pairs[p].a_offset + pairs[p].m);
+        P->need_b = std::max<int64_t>(P->need_b, pairs[p].b_offset + pairs[p].n);
+        P->need_out = std::max<int64_t>(P->need_out, pairs[p].out_offset + pairs[p].m + pairs[p].n);
+    }
+    Schedule S = build_schedule(pairs, npairs, P->tm);
+    P->ntasks = int32_t(S.tasks.size());
+    P->work_bytes = align_up(sizeof(int32_t) * (4 + S.tasks.size()), 256);
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](void **ptr, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(ptr, bytes < 16 ? 16 : bytes);
+    };
+    alloc(reinterpret_cast<void **>(&P->d_pairs), sizeof(PairDev) * size_t(npairs));
+    alloc(reinterpret_cast<void **>(&P->d_tasks), sizeof(int2) * S.tasks.size());
+    alloc(reinterpret_cast<void **>(&P->d_scr_off), sizeof(int64_t) * size_t(npairs));
+    alloc(reinterpret_cast<void **>(&P->d_scratch), sizeof(int32_t) * size_t(S.scratch_elems) + 16);
+    alloc(reinterpret_cast<void **>(&P->d_work), P->work_bytes);
+    if (e == cudaSuccess && npairs)
+        e = cudaMemcpy(P->d_pairs, pairs, sizeof(PairDev) * size_t(npairs), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !S.tasks.empty())
+        e = cudaMemcpy(P->d_tasks, S.tasks.data(), sizeof(int2) * S.tasks.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && npairs)
+        e = cudaMemcpy(P->d_scr_off, S.scratch_off.data(), sizeof(int64_t) * size_t(npairs), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        slcs_batch_plan_destroy(P);
+        return cuda_fail(e, "batch plan upload");
+    }
+    *plan_out = P;
+    return SLCS_OK;
+}
+
+int32_t slcs_batch_plan_launches(const slcs_batch_plan *P)
+{
+    if (!P) return 0;
+    return (P->ntasks > 0 ? 1 : 0) + int32_t(P->empty_pairs.size());
+}
+
+slcs_status slcs_batch_plan_run(slcs_batch_plan *P, const uint8_t *a, const uint8_t *b, int32_t *out, void *stream)
+{
+    if (!P) return fail(SLCS_ERR_INVALID, "plan is null");
+    if (P->npairs > 0 && (!out || (P->ntasks > 0 && (!a || !b))))
+        return fail(SLCS_ERR_INVALID, "null blob or output pointer");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!P->use_graph) return P->enqueue(a, b, out, st);
+    if (!P->gexec || P->g_a != a || P->g_b != b || P->g_out != out) {
+        if (P->gexec) {
+            cudaGraphExecDestroy(P->gexec);
+            P->gexec = nullptr;
+        }
+        if (!P->cap_stream) SLCS_CUDA(cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking));
+        SLCS_CUDA(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal));
+        slcs_status s = P->enqueue(a, b, out, P->cap_stream);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(P->cap_stream, &g);
+        if (s != SLCS_OK) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&P->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+        P->g_a = a;
+        P->g_b = b;
+        P->g_out = out;
+    }
+    SLCS_CUDA(cudaGraphLaunch(P->gexec, st));
+    return SLCS_OK;
+}
+
+slcs_status slcs_batch_plan_run_host(slcs_batch_plan *P, const uint8_t *a, int64_t a_len, const uint8_t *b,
+                                     int64_t b_len, int32_t *out, int64_t out_len, void *stream)
+{
+    if (!P) return fail(SLCS_ERR_INVALID, "plan is null");
+    if (a_len < P->need_a || b_len < P->need_b || out_len < P->need_out)
+        return fail(SLCS_ERR_RANGE, "a host buffer is shorter than the plan's descriptors reach");
+    if ((P->need_a && !a) || (P->need_b && !b) || (P->need_out && !out))
+        return fail(SLCS_ERR_INVALID, "null host buffer");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t ab = align_up(size_t(P->need_a) + 16, 256), bb = align_up(size_t(P->need_b) + 16, 256);
+    const size_t need = ab + bb + sizeof(int32_t) * size_t(P->need_out) + 16;
+    if (need > P->h_stage_bytes) {
+        SLCS_CUDA(cudaStreamSynchronize(st));
+        cudaFree(P->h_stage);
+        P->h_stage = nullptr;
+        P->h_stage_bytes = 0;
+        SLCS_CUDA(cudaMalloc(reinterpret_cast<void **>(&P->h_stage), need));
+        P->h_stage_bytes = need;
+    }
+    uint8_t *da = reinterpret_cast<uint8_t *>(P->h_stage);
+    uint8_t *db = reinterpret_cast<uint8_t *>(P->h_stage + ab);
+    int32_t *dout = reinterpret_cast<int32_t *>(P->h_stage + ab + bb);
+    if (P->need_a) SLCS_CUDA(cudaMemcpyAsync(da, a, size_t(P->need_a), cudaMemcpyHostToDevice, st));
+    if (P->need_b) SLCS_CUDA(cudaMemcpyAsync(db, b, size_t(P->need_b), cudaMemcpyHostToDevice, st));
+    slcs_status s = slcs_batch_plan_run(P, da, db, dout, stream);
+    if (s != SLCS_OK) return s;
+    if (P->need_out)
+        SLCS_CUDA(cudaMemcpyAsync(out, dout, sizeof(int32_t) * size_t(P->need_out), cudaMemcpyDeviceToHost, st));
+    SLCS_CUDA(cudaStreamSynchronize(st));
+    return slcs_device_status(P->device, 1);
+}
+
+slcs_status slcs_batch_plan_destroy(slcs_batch_plan *P)
+{
+    if (!P) return SLCS_OK;
+    if (P->gexec) cudaGraphExecDestroy(P->gexec);
+    if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
+    cudaFree(P->d_pairs);
+    cudaFree(P->d_tasks);
+    cudaFree(P->d_scr_off);
+    cudaFree(P->d_scratch);
+    cudaFree(P->d_work);
+    cudaFree(P->h_stage);
+    delete P;
+    return SLCS_OK;
+}
+
+slcs_status slcs_comb_batch(const slcs_pair_desc *pairs, int32_t npairs, const uint8_t *a_blob,
+                            const uint8_t *b_blob, int32_t *out, const slcs_config *cfg, void *stream)
+{
+    slcs_batch_plan *P = nullptr;
+    slcs_config c{};
+    if (cfg) c = *cfg;
+    c.use_graph = 0;
+    slcs_status s = slcs_batch_plan_create(&P, pairs, npairs, &c);
+    if (s != SLCS_OK) return s;
+    s = slcs_batch_plan_run(P, a_blob, b_blob, out, stream);
+    cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    slcs_batch_plan_destroy(P);
+    if (s != SLCS_OK) return s;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    return SLCS_OK;
+}
+
+slcs_status slcs_comb_batch_host(const slcs_pair_desc *pairs, int32_t npairs, const uint8_t *a_blob, int64_t a_len,
+                                 const uint8_t *b_blob, int64_t b_len, int32_t *out, int64_t out_len,
+                                 const slcs_config *cfg)
+{
+    slcs_status s = check_pairs(pairs, npairs);
+    if (s != SLCS_OK) return s;
+    for (int32_t p = 0; p < npairs; ++p) {
+        const slcs_pair_desc &d = pairs[p];
+        if (d.a_offset + d.m > a_len || d.b_offset + d.n > b_len || d.out_offset + d.m + d.n > out_len)
+            return fail(SLCS_ERR_RANGE, "pair " + std::to_string(p) + " reaches past its blob");
+    }
+    slcs_batch_plan *P = nullptr;
+    s = slcs_batch_plan_create(&P, pairs, npairs, cfg);
+    if (s != SLCS_OK) return s;
+    cudaStream_t st = nullptr;
+    char *buf = nullptr;
+    const size_t ab = align_up(size_t(a_len) + 16, 256), bb = align_up(size_t(b_len) + 16, 256);
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void **>(&buf), ab + bb + sizeof(int32_t) * size_t(out_len), st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(buf, a_blob, size_t(a_len), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(buf + ab, b_blob, size_t(b_len), cudaMemcpyHostToDevice, st);
+    int32_t *dout = reinterpret_cast<int32_t *>(buf + ab + bb);
+    if (e == cudaSuccess) {
+        s = slcs_batch_plan_run(P, reinterpret_cast<uint8_t *>(buf), reinterpret_cast<uint8_t *>(buf + ab), dout, st);
+        if (s == SLCS_OK)
+            e = cudaMemcpyAsync(out, dout, sizeof(int32_t) * size_t(out_len), cudaMemcpyDeviceToHost, st);
+    }
+    if (buf) cudaFreeAsync(buf, st);
+    cudaError_t e2 = st ? cudaStreamSynchronize(st) : cudaSuccess;
+    if (st) cudaStreamDestroy(st);
+    slcs_batch_plan_destroy(P);
+    if (s != SLCS_OK) return s;
+    if (e != cudaSuccess) return cuda_fail(e, "batch host copies");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamSynchronize");
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return slcs_device_status(dev, 1);
+}
+
+slcs_status slcs_strands_to_permutation(const int32_t *h, int32_t m, const int32_t *v, int32_t n,
+                                        int32_t *row_to_col, int32_t *col_to_row, void *stream)
+{
+    if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
+    if ((m > 0 && !h) || (n > 0 && !v)) return fail(SLCS_ERR_INVALID, "null strands");
+    return launch_strands_to_perm(h, m, v, n, row_to_col, col_to_row, static_cast<cudaStream_t>(stream));
+}
+
+// Restates PermutationMatrix::hash (src/permutation_matrix.hpp:192-203): the
+// reference multiplies in signed 64-bit and its build wraps on overflow, so
+// the wrap is reproduced in unsigned arithmetic; % truncates toward zero.
+int64_t slcs_permutation_hash(const int32_t *col_to_row, int32_t size)
+{
+    const int64_t R = 4294967279LL, M = 4294967291LL;
+    int64_t r = 0;
+    for (int32_t i = 0; i < size; ++i) {
+        const uint64_t t = uint64_t(R) * uint64_t(r) + uint64_t(int64_t(col_to_row[i]));
+        r = int64_t(t) % M;
+    }
+    return r;
+}
+
+slcs_status slcs_braid_multiply(const int32_t *, int32_t, const int32_t *, int32_t, int32_t, int32_t, int32_t *,
+                                const slcs_config *, void *)
+{
+    return fail(SLCS_ERR_UNSUPPORTED, "braid multiplication is not built yet");
+}
+
+} // extern "C"

@@ -1,0 +1,320 @@
+// comb.cu -- seaweed combing on sm_100a.
+//
+// Replaces the reference's tiled SYCL solvers (src/lcs_tiled.hpp:10-251, the
+// sub-group wavefront of src/lcs_common.hpp:131-173 and the register tile of
+// src/lcs_common.hpp:59-92) and its host residual fixup
+// (src/lcs_grid.hpp:451-493, src/lcs_residual_fixup.hpp:74-121).
+//
+// Layout of the work
+//   * The grid of a pair has m rows (symbols of a) and n columns (symbols of b).
+//     A v strand enters every column at the top (id m+j) and moves down; an h
+//     strand enters every row at the left (id m-1-r for row r) and moves right.
+//     Cell rule (src/lcs_residual_fixup.hpp:49-54): swap the two strands when
+//     the symbols match or when h > v.
+//   * One warp combs one row stripe of 32*TM rows: lane l keeps rows
+//     [l*TM, l*TM+TM) of the stripe -- their symbols and h strands -- in
+//     registers for the whole stripe.  Columns advance in blocks of 4; at step
+//     t lane l combs block t-l, so the warp is a 32-deep systolic pipeline and
+//     the 4 v strands of a block travel lane to lane with __shfl_up_sync.
+//   * Lane 31's output is the bottom edge of the stripe.  For the last stripe it
+//     is the final v; otherwise it is written to a per-pair scratch row in HBM
+//     and a progress counter is released every 8 blocks.  Lane 0 of the next
+//     stripe (another warp, usually on another SM) acquires that counter and
+//     streams the row back with 16-byte cp.async.cg copies, 4 blocks ahead.
+//     The scratch row is reused in place: stripe s+1 overwrites block c only
+//     after it has read block c.
+//   * Warps take stripes from a global ticket counter.  Stripes of one pair
+//     have consecutive tickets, so a stripe's producer was claimed earlier by
+//     a running warp and every wait ends; each wait is additionally bounded by
+//     %globaltimer and raises DEV_ERR_TIMEOUT instead of hanging.
+//   * Rows past m and columns past n are masked by data, not by branches:
+//     a masked row has symbol -1 and h = INT_MIN (never swaps), a masked column
+//     has symbol -2 and v = INT_MAX (never swaps), so edge tiles need no host
+//     fixup.
+#include <climits>
+#include <mutex>
+
+#include "comb.cuh"
+
+namespace slcs {
+
+namespace {
+
+constexpr int TN = 4;      // columns per block (one 16-byte v vector)
+constexpr int PREF = 4;    // blocks lane 0 prefetches ahead
+constexpr int RING = 8;    // shared-memory ring slots per warp (> PREF)
+constexpr int PUBLISH = 8; // blocks between progress releases
+
+struct StripeWait {
+    const int32_t *prog;
+    int32_t *abort_flag;
+    uint32_t *status;
+    int32_t avail;
+    uint64_t t0;
+    bool dead;
+
+    // Lane 0 only: wait until the producer has published block `blk`.
+    __device__ __forceinline__ void until(int blk)
+    {
+        if (avail > blk || dead) return;
+        for (;;) {
+            avail = ld_acquire_gpu(prog);
+            if (avail > blk) return;
+            if (ld_relaxed_gpu(abort_flag)) {
+                dead = true;
+                return;
+            }
+            uint64_t now = globaltimer_ns();
+            if (t0 == 0) {
+                t0 = now;
+            } else if (now - t0 > WAIT_LIMIT_NS) {
+                dead = true;
+                st_relaxed_gpu(abort_flag, 1);
+                raise_status(status, DEV_ERR_TIMEOUT);
+                return;
+            }
+            __nanosleep(128);
+        }
+    }
+};
+
+__device__ __forceinline__ void cell(int a_sym, int b_sym, int &h, int &v)
+{
+    const bool swap = (a_sym == b_sym) | (h > v);
+    const int nh = swap ? v : h;
+    v = swap ? h : v;
+    h = nh;
+}
+
+template <int TM>
+__device__ __forceinline__ void comb_stripe(const CombLaunch &L, const PairDev &P, int64_t scr_off,
+                                            int stripe, int task, int4 *ring, int lane)
+{
+    const int m = P.m, n = P.n;
+    const uint8_t *__restrict__ a = L.a_blob + P.a_off;
+    const uint8_t *__restrict__ b = L.b_blob + P.b_off;
+    int32_t *hout = L.out + P.out_off;
+    int32_t *vout = hout + m;
+    int32_t *scr = L.scratch + scr_off;
+
+    const int r0 = stripe * 32 * TM;
+    int av[TM], hv[TM];
+#pragma unroll
+    for (int k = 0; k < TM; ++k) {
+        const int r = r0 + lane * TM + k;
+        const bool in = r < m;
+        av[k] = in ? int(a[r]) : -1;
+        hv[k] = in ? (m - 1 - r) : INT_MIN;
+    }
+    const bool first = stripe == 0;
+    const bool has_next = r0 + 32 * TM < m;
+    const int nb = (n + TN - 1) / TN;
+    const bool b_aligned = (reinterpret_cast<uintptr_t>(b) & 3) == 0;
+
+    StripeWait W{L.progress + (task - 1), L.counters + 1, L.status, 0, 0, false};
+    int32_t *prog_mine = L.progress + task;
+
+    if (!first && lane == 0) {
+#pragma unroll
+        for (int d = 0; d < PREF; ++d) {
+            if (d < nb) {
+                W.until(d);
+                if (!W.dead) cp_async_cg16(&ring[d], scr + d * TN);
+            }
+            cp_async_commit();
+        }
+    }
+
+    int vc[TN];
+#pragma unroll
+    for (int j = 0; j < TN; ++j) vc[j] = INT_MAX;
+
+    const int steps = nb + 31;
+    for (int t = 0; t < steps; ++t) {
+        const int blk = t - lane;
+        const bool act = unsigned(blk) < unsigned(nb);
+
+        int vi[TN];
+#pragma unroll
+        for (int j = 0; j < TN; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1);
+
+        if (lane == 0) {
+            if (t < nb) {
+                const int c = t * TN;
+                if (first) {
+#pragma unroll
+                    for (int j = 0; j < TN; ++j) vi[j] = (c + j < n) ? m + c + j : INT_MAX;
+                } else {
+                    const int nxt = t + PREF;
+                    if (nxt < nb) {
+                        W.until(nxt);
+                        if (!W.dead) cp_async_cg16(&ring[nxt & (RING - 1)], scr + nxt * TN);
+                    }
+                    cp_async_commit();
+                    cp_async_wait<PREF>();
+                    const int4 x = ring[t & (RING - 1)];
+                    vi[0] = x.x;
+                    vi[1] = x.y;
+                    vi[2] = x.z;
+                    vi[3] = x.w;
+                    if (c + TN > n) {
+#pragma unroll
+                        for (int j = 0; j < TN; ++j)
+                            if (c + j >= n) vi[j] = INT_MAX;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < TN; ++j) vi[j] = INT_MAX;
+            }
+        }
+
+        int bs[TN];
+        if (act) {
+            const int c = blk * TN;
+            if (b_aligned && c + TN <= n) {
+                const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(b + c));
+#pragma unroll
+                for (int j = 0; j < TN; ++j) bs[j] = int((w >> (8 * j)) & 0xffu);
+            } else {
+#pragma unroll
+                for (int j = 0; j < TN; ++j) bs[j] = (c + j < n) ? int(__ldg(b + c + j)) : -2;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < TN; ++j) bs[j] = -2;
+        }
+
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+            int v = vi[j];
+#pragma unroll
+            for (int k = 0; k < TM; ++k) cell(av[k], bs[j], hv[k], v);
+            vc[j] = v;
+        }
+
+        if (lane == 31 && act) {
+            const int c = blk * TN;
+            if (has_next) {
+                *reinterpret_cast<int4 *>(scr + c) = make_int4(vc[0], vc[1], vc[2], vc[3]);
+                if ((blk & (PUBLISH - 1)) == PUBLISH - 1 || blk == nb - 1) st_release_gpu(prog_mine, blk + 1);
+            } else {
+#pragma unroll
+                for (int j = 0; j < TN; ++j)
+                    if (c + j < n) vout[c + j] = vc[j];
+            }
+        }
+    }
+    if (!first && lane == 0) cp_async_wait<0>();
+
+#pragma unroll
+    for (int k = 0; k < TM; ++k) {
+        const int r = r0 + lane * TM + k;
+        if (r < m) hout[m - 1 - r] = hv[k];
+    }
+}
+
+template <int TM, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) comb_wavefront_kernel(const CombLaunch L)
+{
+    __shared__ __align__(16) int4 ring[WARPS][RING];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    for (;;) {
+        int k = 0;
+        if (lane == 0) k = ld_relaxed_gpu(L.counters + 1) ? INT_MAX : atomicAdd(L.counters, 1);
+        k = __shfl_sync(FULL_MASK, k, 0);
+        if (k >= L.ntasks) break;
+        PairDev P;
+        int stripe;
+        int64_t so = 0;
+        if (L.tasks) {
+            const int2 tk = L.tasks[k];
+            P = L.pairs[tk.x];
+            stripe = tk.y;
+            so = L.scratch_off[tk.x];
+        } else {
+            P = L.single;
+            stripe = k;
+        }
+        comb_stripe<TM>(L, P, so, stripe, k, ring[w], lane);
+    }
+}
+
+__global__ void strands_to_perm_kernel(const int32_t *__restrict__ h, int32_t m, const int32_t *__restrict__ v,
+                                       int32_t n, int32_t *r2c, int32_t *c2r)
+{
+    const int32_t size = m + n;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < size; i += gridDim.x * blockDim.x) {
+        const int32_t id = i < m ? h[i] : v[i - m];
+        const int32_t col = i < m ? n + i : i - m;
+        if (id >= 0 && id < size) {
+            if (r2c) r2c[id] = col;
+            if (c2r) c2r[col] = id;
+        }
+    }
+}
+
+template <int TM, int WARPS>
+slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_out)
+{
+    static int occ = -1;
+    static std::mutex mu;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (occ < 0) {
+            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WARPS>,
+                                                                    WARPS * 32, 0));
+            if (occ < 1) occ = 1;
+        }
+    }
+    const long want = (long(L.ntasks) + WARPS - 1) / WARPS;
+    long grid = long(sm_count()) * occ;
+    if (want < grid) grid = want;
+    if (grid < 1) grid = 1;
+    comb_wavefront_kernel<TM, WARPS><<<int(grid), WARPS * 32, 0, stream>>>(L);
+    if (grid_out) *grid_out = int(grid);
+    SLCS_CUDA(cudaGetLastError());
+    return SLCS_OK;
+}
+
+} // namespace
+
+bool tile_m_supported(int tm) { return tm == 2 || tm == 4 || tm == 8 || tm == 12 || tm == 16; }
+int rows_per_stripe(int tm) { return 32 * tm; }
+
+slcs_status launch_comb(const CombLaunch &L, int tile_m, int warps, cudaStream_t stream, int *grid_out)
+{
+    if (L.ntasks <= 0) return SLCS_OK;
+#define SLCS_TM_CASE(TM)                                                                   \
+    case TM:                                                                               \
+        if (warps == 2) return launch_variant<TM, 2>(L, stream, grid_out);                 \
+        if (warps == 8) return launch_variant<TM, 8>(L, stream, grid_out);                 \
+        return launch_variant<TM, 4>(L, stream, grid_out);
+    switch (tile_m) {
+        SLCS_TM_CASE(2)
+        SLCS_TM_CASE(4)
+        SLCS_TM_CASE(8)
+        SLCS_TM_CASE(12)
+        SLCS_TM_CASE(16)
+    default:
+        return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+    }
+#undef SLCS_TM_CASE
+}
+
+slcs_status launch_strands_to_perm(const int32_t *h, int32_t m, const int32_t *v, int32_t n, int32_t *r2c,
+                                   int32_t *c2r, cudaStream_t stream)
+{
+    const int64_t size = int64_t(m) + n;
+    if (size <= 0) return SLCS_OK;
+    if (r2c) SLCS_CUDA(cudaMemsetAsync(r2c, 0xff, size * sizeof(int32_t), stream));
+    if (c2r) SLCS_CUDA(cudaMemsetAsync(c2r, 0xff, size * sizeof(int32_t), stream));
+    int blocks = int((size + 255) / 256);
+    if (blocks > sm_count() * 8) blocks = sm_count() * 8;
+    strands_to_perm_kernel<<<blocks, 256, 0, stream>>>(h, m, v, n, r2c, c2r);
+    SLCS_CUDA(cudaGetLastError());
+    return SLCS_OK;
+}
+
+} // namespace slcs

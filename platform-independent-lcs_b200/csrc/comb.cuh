@@ -1,0 +1,45 @@
+// comb.cuh -- host-side interface of the seaweed-combing kernels.
+#pragma once
+
+#include "slcs_internal.cuh"
+
+namespace slcs {
+
+// Everything one launch of the combing kernel reads.  A "task" is one row
+// stripe (32 * tile_m rows of a) of one pair combed across all of b.  Stripes
+// of a pair are consecutive tasks in ascending order, so the producer of task
+// k (stripe s > 0) is task k-1, which a running warp always claimed first.
+struct CombLaunch {
+    const PairDev *pairs;       // device; null = single pair in `single`
+    const int2 *tasks;          // device (pair, stripe); null = stripe k of `single`
+    int32_t ntasks;
+    const uint8_t *a_blob;
+    const uint8_t *b_blob;
+    int32_t *out;               // h then v of every pair (offsets in PairDev)
+    int32_t *scratch;           // inter-stripe v strands, 16-byte aligned per pair
+    const int64_t *scratch_off; // device, per pair; null = 0 for `single`
+    int32_t *progress;          // ntasks counters (blocks of 4 columns published)
+    int32_t *counters;          // [0] ticket, [1] abort flag
+    uint32_t *status;           // mapped device status word
+    PairDev single;
+};
+
+// Rows of a one lane keeps in registers; supported values.
+bool tile_m_supported(int tm);
+int rows_per_stripe(int tm);
+// Stripes of a pair with m rows.
+inline int32_t stripes_of(int32_t m, int tm) { return m <= 0 ? 0 : (m + 32 * tm - 1) / (32 * tm); }
+// Scratch elements a pair needs (0 when it has a single stripe).
+inline int64_t scratch_elems(int32_t m, int32_t n, int tm)
+{
+    return stripes_of(m, tm) > 1 ? (int64_t(n) + 3) / 4 * 4 : 0;
+}
+
+// Enqueue one persistent launch; `counters` and `progress` must be zero.
+slcs_status launch_comb(const CombLaunch &L, int tile_m, int warps, cudaStream_t stream, int *grid_out);
+
+// Strands -> permutation matrix arrays (either output may be null).
+slcs_status launch_strands_to_perm(const int32_t *h, int32_t m, const int32_t *v, int32_t n,
+                                   int32_t *row_to_col, int32_t *col_to_row, cudaStream_t stream);
+
+} // namespace slcs

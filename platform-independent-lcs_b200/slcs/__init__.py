@@ -1,0 +1,239 @@
+"""Python binding of libslcs.so (the B200 semi-local LCS engine).
+
+The binding is a thin ctypes layer over the C ABI declared in include/slcs.h.
+There is no CPU fallback: if the CUDA library is missing, every entry point
+raises.  Device buffers are torch CUDA tensors (torch is used for device
+memory and streams only); host buffers are numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+ROOT_DIR = os.path.dirname(PKG_DIR)
+LIB_PATH = os.path.join(ROOT_DIR, "lib", "libslcs.so")
+
+ALGO_AUTO, ALGO_WAVEFRONT, ALGO_STRIPS = 0, 1, 2
+
+
+class SlcsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"slcs status {status}: {message}")
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("algo", ctypes.c_int32), ("tile_m", ctypes.c_int32), ("tile_n", ctypes.c_int32),
+                ("warps", ctypes.c_int32), ("braid_cutoff", ctypes.c_int32), ("strips", ctypes.c_int32),
+                ("use_graph", ctypes.c_int32), ("reserved", ctypes.c_int32 * 9)]
+
+    @classmethod
+    def make(cls, **kw) -> "Config":
+        c = cls()
+        for k, v in kw.items():
+            if v is not None:
+                setattr(c, k, int(v))
+        return c
+
+
+class PairDesc(ctypes.Structure):
+    _fields_ = [("a_offset", ctypes.c_int64), ("b_offset", ctypes.c_int64), ("out_offset", ctypes.c_int64),
+                ("m", ctypes.c_int32), ("n", ctypes.c_int32)]
+
+
+PAIR_DTYPE = np.dtype([("a_offset", np.int64), ("b_offset", np.int64), ("out_offset", np.int64),
+                       ("m", np.int32), ("n", np.int32)])
+
+_LIB = None
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+
+
+def lib():
+    """Load libslcs.so; raise if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libslcs.so not found at {LIB_PATH}: run __graft_entry__.build() "
+                               f"(make -C platform-independent-lcs_b200)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.slcs_last_error.restype = ctypes.c_char_p
+        L.slcs_status_string.restype = ctypes.c_char_p
+        L.slcs_status_string.argtypes = [_i32]
+        L.slcs_device_status.argtypes = [_i32, _i32]
+        L.slcs_version.restype = _i32
+        L.slcs_comb_pair.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, ctypes.POINTER(Config), _vp]
+        L.slcs_comb_pair_host.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, ctypes.POINTER(Config)]
+        L.slcs_comb_batch.argtypes = [_vp, _i32, _vp, _vp, _vp, ctypes.POINTER(Config), _vp]
+        L.slcs_comb_batch_host.argtypes = [_vp, _i32, _vp, _i64, _vp, _i64, _vp, _i64, ctypes.POINTER(Config)]
+        L.slcs_batch_plan_create.argtypes = [ctypes.POINTER(_vp), _vp, _i32, ctypes.POINTER(Config)]
+        L.slcs_batch_plan_run.argtypes = [_vp, _vp, _vp, _vp, _vp]
+        L.slcs_batch_plan_destroy.argtypes = [_vp]
+        L.slcs_batch_plan_run_host.argtypes = [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp]
+        L.slcs_batch_plan_launches.argtypes = [_vp]
+        L.slcs_batch_plan_launches.restype = _i32
+        L.slcs_strands_to_permutation.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, _vp]
+        L.slcs_permutation_hash.argtypes = [_vp, _i32]
+        L.slcs_permutation_hash.restype = _i64
+        L.slcs_probe_int_rates.argtypes = [_i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _vp]
+        L.slcs_braid_multiply.argtypes = [_vp, _i32, _vp, _i32, _i32, _i32, _vp, ctypes.POINTER(Config), _vp]
+        _LIB = L
+    return _LIB
+
+
+def check(status: int):
+    if status != 0:
+        msg = lib().slcs_last_error().decode(errors="replace")
+        raise SlcsError(status, msg)
+
+
+def _cfg(cfg: Optional[Config]):
+    return ctypes.byref(cfg) if cfg is not None else None
+
+
+def _stream(stream) -> Optional[int]:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _dptr(t) -> int:
+    return t.data_ptr() if t is not None and t.numel() > 0 else 0
+
+
+def device_status(device: int = 0, clear: bool = True):
+    check(lib().slcs_device_status(device, int(clear)))
+
+
+# ---------------------------------------------------------------------------
+# combing
+# ---------------------------------------------------------------------------
+
+def comb_pair(a, b, cfg: Optional[Config] = None, stream=None, out=None):
+    """Strands of one pair.  a, b: uint8 CUDA tensors.  Returns (h, v) int32
+    CUDA views into one contiguous buffer (h first, as the C ABI lays it out)."""
+    import torch
+    m, n = int(a.numel()), int(b.numel())
+    if out is None:
+        out = torch.empty(m + n, dtype=torch.int32, device=a.device)
+    h, v = out[:m], out[m:]
+    check(lib().slcs_comb_pair(_dptr(a), m, _dptr(b), n, _dptr(out), _dptr(out) + 4 * m if n else 0,
+                               _cfg(cfg), _stream(stream)))
+    return h, v
+
+
+def comb_pair_host(a: np.ndarray, b: np.ndarray, cfg: Optional[Config] = None):
+    """Strands of one pair from host numpy arrays (synchronous)."""
+    a = np.ascontiguousarray(a, np.uint8)
+    b = np.ascontiguousarray(b, np.uint8)
+    h = np.empty(len(a), np.int32)
+    v = np.empty(len(b), np.int32)
+    check(lib().slcs_comb_pair_host(a.ctypes.data, len(a), b.ctypes.data, len(b), h.ctypes.data,
+                                    v.ctypes.data, _cfg(cfg)))
+    return h, v
+
+
+def pair_descs(batch) -> np.ndarray:
+    """slcs_pair_desc array for a workloads.Batch (strands packed h then v)."""
+    off, _ = batch.strand_offsets()
+    d = np.zeros(batch.npairs, PAIR_DTYPE)
+    d["a_offset"] = batch.a_off
+    d["b_offset"] = batch.b_off
+    d["out_offset"] = off
+    d["m"] = batch.ms
+    d["n"] = batch.ns
+    return d
+
+
+class BatchPlan:
+    """Reusable schedule of one batch (C ABI slcs_batch_plan)."""
+
+    def __init__(self, descs: np.ndarray, cfg: Optional[Config] = None):
+        self._descs = np.ascontiguousarray(descs, PAIR_DTYPE)
+        self._h = _vp()
+        check(lib().slcs_batch_plan_create(ctypes.byref(self._h), self._descs.ctypes.data, len(self._descs),
+                                           _cfg(cfg)))
+
+    @property
+    def launches(self) -> int:
+        return int(lib().slcs_batch_plan_launches(self._h))
+
+    def run(self, a_blob, b_blob, out, stream=None):
+        check(lib().slcs_batch_plan_run(self._h, _dptr(a_blob), _dptr(b_blob), _dptr(out), _stream(stream)))
+
+    def run_host(self, a_blob: np.ndarray, b_blob: np.ndarray, out: np.ndarray, stream=None):
+        """Host buffers in and out (pinned buffers make the copies asynchronous)."""
+        check(lib().slcs_batch_plan_run_host(self._h, a_blob.ctypes.data, a_blob.size, b_blob.ctypes.data,
+                                             b_blob.size, out.ctypes.data, out.size, _stream(stream)))
+
+    def close(self):
+        if self._h:
+            lib().slcs_batch_plan_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def comb_batch(descs: np.ndarray, a_blob, b_blob, out, cfg: Optional[Config] = None, stream=None):
+    descs = np.ascontiguousarray(descs, PAIR_DTYPE)
+    check(lib().slcs_comb_batch(descs.ctypes.data, len(descs), _dptr(a_blob), _dptr(b_blob), _dptr(out),
+                                _cfg(cfg), _stream(stream)))
+
+
+def comb_batch_host(descs: np.ndarray, a_blob: np.ndarray, b_blob: np.ndarray, out_len: int,
+                    cfg: Optional[Config] = None, out: Optional[np.ndarray] = None) -> np.ndarray:
+    descs = np.ascontiguousarray(descs, PAIR_DTYPE)
+    a_blob = np.ascontiguousarray(a_blob, np.uint8)
+    b_blob = np.ascontiguousarray(b_blob, np.uint8)
+    if out is None:
+        out = np.empty(out_len, np.int32)
+    check(lib().slcs_comb_batch_host(descs.ctypes.data, len(descs), a_blob.ctypes.data, len(a_blob),
+                                     b_blob.ctypes.data, len(b_blob), out.ctypes.data, out_len, _cfg(cfg)))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# permutation matrix and braid multiplication
+# ---------------------------------------------------------------------------
+
+def strands_to_permutation(h, v, stream=None):
+    import torch
+    m, n = int(h.numel()), int(v.numel())
+    r2c = torch.empty(m + n, dtype=torch.int32, device=h.device)
+    c2r = torch.empty(m + n, dtype=torch.int32, device=h.device)
+    check(lib().slcs_strands_to_permutation(_dptr(h), m, _dptr(v), n, _dptr(r2c), _dptr(c2r), _stream(stream)))
+    return r2c, c2r
+
+
+def permutation_hash(col_to_row: np.ndarray) -> int:
+    c = np.ascontiguousarray(col_to_row, np.int32)
+    return int(lib().slcs_permutation_hash(c.ctypes.data, len(c)))
+
+
+def braid_multiply(p_r2c, q_r2c, k: int, row_glue: bool, cfg: Optional[Config] = None, stream=None):
+    import torch
+    size = int(p_r2c.numel()) + int(q_r2c.numel()) - int(k)
+    out = torch.empty(size, dtype=torch.int32, device=p_r2c.device)
+    check(lib().slcs_braid_multiply(_dptr(p_r2c), int(p_r2c.numel()), _dptr(q_r2c), int(q_r2c.numel()), int(k),
+                                    int(bool(row_glue)), _dptr(out), _cfg(cfg), _stream(stream)))
+    return out
+
+
+def probe_int_rates(iters: int = 4096, stream=None):
+    """(INT32 min/max ops per second, register-only cell updates per second)."""
+    ops = ctypes.c_double()
+    cells = ctypes.c_double()
+    check(lib().slcs_probe_int_rates(int(iters), ctypes.byref(ops), ctypes.byref(cells), _stream(stream)))
+    return ops.value, cells.value

@@ -1,0 +1,146 @@
+"""Parity of the CUDA combing kernels with the CPU oracle (bit-exact strands)."""
+import numpy as np
+import pytest
+
+import oracle as O
+import slcs
+from slcs import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(x, device):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).to(device)
+
+
+def _check_pair(a, b, device, cfg=None):
+    h, v = slcs.comb_pair(_dev(a, device), _dev(b, device), cfg=cfg)
+    import torch
+    torch.cuda.synchronize()
+    slcs.device_status(0)
+    eh, ev = O.comb(a, b)
+    np.testing.assert_array_equal(h.cpu().numpy(), eh)
+    np.testing.assert_array_equal(v.cpu().numpy(), ev)
+
+
+SHAPES = [(1, 1), (1, 7), (7, 1), (2, 3), (31, 33), (32, 32), (33, 4), (64, 129), (127, 255),
+          (257, 100), (500, 3), (3, 500), (1000, 1001), (1023, 517), (2049, 2047)]
+
+
+@pytest.mark.parametrize("tm", [2, 4, 8, 12, 16])
+def test_pair_shapes(cuda, tm):
+    rng = np.random.default_rng(10 + tm)
+    for (m, n) in SHAPES:
+        sigma = int(rng.choice([2, 4, 20, 256]))
+        a = rng.integers(0, sigma, m, dtype=np.uint8)
+        b = rng.integers(0, sigma, n, dtype=np.uint8)
+        _check_pair(a, b, cuda, slcs.Config.make(tile_m=tm))
+
+
+@pytest.mark.parametrize("warps", [2, 4, 8])
+def test_pair_warps(cuda, warps):
+    rng = np.random.default_rng(warps)
+    a = rng.integers(0, 4, 3000, dtype=np.uint8)
+    b = rng.integers(0, 4, 2500, dtype=np.uint8)
+    _check_pair(a, b, cuda, slcs.Config.make(tile_m=2, warps=warps))
+
+
+def test_pair_4096_golden(cuda):
+    a, b = W.pair_4096()
+    h, v = slcs.comb_pair(_dev(a, cuda), _dev(b, cuda))
+    r2c, c2r = slcs.strands_to_permutation(h, v)
+    c2r = c2r.cpu().numpy()
+    eh, ev = O.comb(a, b)
+    er2c, ec2r = O.from_strands(eh, ev)
+    np.testing.assert_array_equal(c2r, ec2r)
+    np.testing.assert_array_equal(r2c.cpu().numpy(), er2c)
+    assert slcs.permutation_hash(c2r) == O.perm_hash(ec2r)
+
+
+def test_test_default_hashes(cuda):
+    """The reference's own test script cases (test_default.txt) by hash."""
+    for (m, n, want) in [(7330, 9944, 944438867), (9771, 11302, 2348829537), (19771, 24302, 3164269182)]:
+        a = O.mt19937_binary(m, 888)
+        b = O.mt19937_binary(n, 999)
+        h, v = slcs.comb_pair(_dev(a, cuda), _dev(b, cuda))
+        _, c2r = slcs.strands_to_permutation(h, v)
+        assert slcs.permutation_hash(c2r.cpu().numpy()) == want
+
+
+def test_pair_unaligned_and_split_outputs(cuda):
+    import torch
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, 4, 777, dtype=np.uint8)
+    b = rng.integers(0, 4, 901, dtype=np.uint8)
+    abuf = _dev(np.concatenate([[9], a]).astype(np.uint8), cuda)
+    bbuf = _dev(np.concatenate([[9, 9, 9], b]).astype(np.uint8), cuda)
+    h = torch.empty(777, dtype=torch.int32, device=cuda)
+    v = torch.empty(901, dtype=torch.int32, device=cuda)
+    L = slcs.lib()
+    slcs.check(L.slcs_comb_pair(abuf.data_ptr() + 1, 777, bbuf.data_ptr() + 3, 901, h.data_ptr(), v.data_ptr(),
+                                None, torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    eh, ev = O.comb(a, b)
+    np.testing.assert_array_equal(h.cpu().numpy(), eh)
+    np.testing.assert_array_equal(v.cpu().numpy(), ev)
+
+
+def test_pair_empty_sides(cuda):
+    for (m, n) in [(0, 5), (5, 0), (0, 0)]:
+        h, v = slcs.comb_pair_host(np.zeros(m, np.uint8), np.zeros(n, np.uint8))
+        np.testing.assert_array_equal(h, np.arange(m))
+        np.testing.assert_array_equal(v, np.arange(m, m + n))
+
+
+def test_pair_host_api(cuda):
+    rng = np.random.default_rng(4)
+    a = rng.integers(0, 20, 1500, dtype=np.uint8)
+    b = rng.integers(0, 20, 1700, dtype=np.uint8)
+    h, v = slcs.comb_pair_host(a, b)
+    eh, ev = O.comb(a, b)
+    np.testing.assert_array_equal(h, eh)
+    np.testing.assert_array_equal(v, ev)
+
+
+def _batch_expected(batch):
+    off, total = batch.strand_offsets()
+    return O.comb_batch(batch.a_blob, batch.b_blob, batch.a_off, batch.b_off, batch.ms, batch.ns, off, total)
+
+
+@pytest.mark.parametrize("graph", [0, 1])
+def test_batch_reads(cuda, graph):
+    import torch
+    batch = W.reads_20000(npairs=3000)
+    descs = slcs.pair_descs(batch)
+    _, total = batch.strand_offsets()
+    out = torch.empty(total, dtype=torch.int32, device=cuda)
+    plan = slcs.BatchPlan(descs, slcs.Config.make(use_graph=graph))
+    a_d, b_d = _dev(batch.a_blob, cuda), _dev(batch.b_blob, cuda)
+    want = _batch_expected(batch)
+    for _ in range(2):
+        out.fill_(-7)
+        plan.run(a_d, b_d, out)
+        torch.cuda.synchronize()
+        slcs.device_status(0)
+        np.testing.assert_array_equal(out.cpu().numpy(), want)
+
+
+def test_batch_mixed_sizes(cuda):
+    import torch
+    rng = np.random.default_rng(11)
+    pairs = []
+    for _ in range(300):
+        m = int(rng.integers(0, 1500)); n = int(rng.integers(0, 1500))
+        sigma = int(rng.choice([2, 4, 256]))
+        pairs.append((rng.integers(0, sigma, m, dtype=np.uint8), rng.integers(0, sigma, n, dtype=np.uint8)))
+    batch = W.pack(pairs)
+    descs = slcs.pair_descs(batch)
+    _, total = batch.strand_offsets()
+    for tm in (2, 8, 16):
+        out = torch.full((total,), -7, dtype=torch.int32, device=cuda)
+        slcs.comb_batch(descs, _dev(batch.a_blob, cuda), _dev(batch.b_blob, cuda), out, slcs.Config.make(tile_m=tm))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy(), _batch_expected(batch))
+    host = slcs.comb_batch_host(descs, batch.a_blob, batch.b_blob, total)
+    np.testing.assert_array_equal(host, _batch_expected(batch))
