@@ -282,7 +282,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": "reads_20000", "pairs_per_gpu": batch.npairs, "cells_per_gpu_step": batch.cells,
-                   "variant": {"tile_m": plan_tile_m(cfg), "warps": cfg.warps or 4, "graph": bool(cfg.use_graph)},
+                   "variant": dict(plan.info, graph=bool(cfg.use_graph)),
                    "tuned_by": tuned_by, "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"{world} independent batches (weak)"},
         "e2e": e2e,
@@ -305,10 +305,6 @@ def main():
         pg.barrier()
         pg.destroy_process_group()
     return 0
-
-
-def plan_tile_m(cfg):
-    return cfg.tile_m or 8
 
 
 if __name__ == "__main__":

@@ -63,7 +63,9 @@ typedef struct {
     int32_t braid_cutoff;  /* steady-ant size below which one block finishes a node   */
     int32_t strips;        /* column strips for SLCS_ALGO_STRIPS                      */
     int32_t use_graph;     /* batch plans: replay the launch as a captured CUDA graph */
-    int32_t reserved[9];
+    int32_t seg;           /* batch stream mode: lanes per pipeline segment (8/16/32) */
+    int32_t wait_ms;       /* limit of one device-side wait (default 10000 ms)        */
+    int32_t reserved[7];
 } slcs_config;
 
 /* One pair of a batch: symbols at a_blob[a_offset .. +m) and b_blob[b_offset .. +n);
@@ -135,6 +137,18 @@ SLCS_API slcs_status slcs_batch_plan_run_host(slcs_batch_plan *plan, const uint8
 SLCS_API slcs_status slcs_batch_plan_destroy(slcs_batch_plan *plan);
 /* Kernel launches one slcs_batch_plan_run issues (for launch accounting). */
 SLCS_API int32_t slcs_batch_plan_launches(const slcs_batch_plan *plan);
+
+/* What a plan decided: the kernel variant and how the pairs were split. */
+typedef struct {
+    int32_t stream_tile_m;   /* rows per lane of streamed pairs (0: wavefront only) */
+    int32_t seg;             /* lanes per stream segment                            */
+    int32_t wavefront_tile_m;/* rows per lane of wavefront stripes                  */
+    int32_t warps;           /* warps per block                                     */
+    int32_t stream_pairs;    /* pairs combed in stream mode                         */
+    int32_t wavefront_tasks; /* row stripes combed as wavefront tasks               */
+    int32_t reserved[2];
+} slcs_plan_info;
+SLCS_API slcs_status slcs_batch_plan_info(const slcs_batch_plan *plan, slcs_plan_info *info);
 
 /* ---- permutation matrix ------------------------------------------------ */
 

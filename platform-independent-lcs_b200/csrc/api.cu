@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "braid.cuh"
 #include "comb.cuh"
 
 namespace slcs {
@@ -73,15 +74,18 @@ __global__ void identity_strands_kernel(int32_t *h, int32_t m, int32_t *v, int32
     }
 }
 
-// Host schedule of a batch: pairs ordered by cells (largest first), each
-// pair's stripes as consecutive tasks, scratch rows for multi-stripe pairs.
+// Host schedule of a batch: pairs ordered by cells (largest first).  Pairs of
+// at most stream_rows rows (stream_rows > 0) are streamed; every other pair
+// contributes its row stripes as consecutive wavefront tasks, with a scratch
+// row when it has more than one stripe.
 struct Schedule {
     std::vector<int2> tasks;
+    std::vector<int32_t> stream_pairs;
     std::vector<int64_t> scratch_off;
     int64_t scratch_elems = 0;
 };
 
-Schedule build_schedule(const slcs_pair_desc *pairs, int32_t npairs, int tm)
+Schedule build_schedule(const slcs_pair_desc *pairs, int32_t npairs, int tm, int32_t stream_rows)
 {
     Schedule S;
     std::vector<int32_t> order(npairs);
@@ -91,7 +95,12 @@ Schedule build_schedule(const slcs_pair_desc *pairs, int32_t npairs, int tm)
     });
     S.scratch_off.assign(npairs, 0);
     for (int32_t p : order) {
-        const int32_t st = (pairs[p].n > 0) ? stripes_of(pairs[p].m, tm) : 0;
+        if (pairs[p].m == 0 || pairs[p].n == 0) continue;
+        if (pairs[p].m <= stream_rows) {
+            S.stream_pairs.push_back(p);
+            continue;
+        }
+        const int32_t st = stripes_of(pairs[p].m, tm);
         for (int32_t s = 0; s < st; ++s) S.tasks.push_back(make_int2(p, s));
         const int64_t e = scratch_elems(pairs[p].m, pairs[p].n, tm);
         if (e) {
@@ -147,12 +156,17 @@ using namespace slcs;
 
 struct slcs_batch_plan {
     int device = 0;
-    int tm = 8;
+    int tm = 8;      // rows per lane of the wavefront tasks
     int warps = 4;
+    int stm = 0;     // rows per lane in stream mode (0: wavefront only)
+    int seg = 16;    // lanes per stream segment
     int32_t npairs = 0;
     int32_t ntasks = 0;
+    int32_t nstream = 0;
+    uint64_t wait_ns = DEFAULT_WAIT_NS;
     bool use_graph = false;
     PairDev *d_pairs = nullptr;
+    int32_t *d_stream = nullptr;
     int2 *d_tasks = nullptr;
     int64_t *d_scr_off = nullptr;
     int32_t *d_scratch = nullptr;
@@ -182,13 +196,20 @@ struct slcs_batch_plan {
         L.counters = d_work;
         L.progress = d_work + 4;
         L.status = device_status_word();
+        L.wait_ns = wait_ns;
         return L;
     }
 
     slcs_status enqueue(const uint8_t *a, const uint8_t *b, int32_t *out, cudaStream_t st) const
     {
         SLCS_CUDA(cudaMemsetAsync(d_work, 0, work_bytes, st));
-        slcs_status s = launch_comb(launch(a, b, out), tm, warps, st, nullptr);
+        slcs_status s;
+        if (stm > 0) {
+            BatchLaunch B{launch(a, b, out), d_stream, nstream};
+            s = launch_batch(B, stm, seg, st, nullptr);
+        } else {
+            s = launch_comb(launch(a, b, out), tm, warps, st, nullptr);
+        }
         if (s != SLCS_OK) return s;
         for (const auto &d : empty_pairs) {
             s = write_identity(out + d.out_offset, d.m, out + d.out_offset + d.m, d.n, st);
@@ -249,6 +270,7 @@ slcs_status slcs_device_status(int32_t device, int32_t clear)
     if (clear && s.host_status) __atomic_store_n(s.host_status, 0u, __ATOMIC_SEQ_CST);
     if (device != cur) cudaSetDevice(cur);
     if (bits & DEV_ERR_TIMEOUT) return fail(SLCS_ERR_TIMEOUT, "a device-side wait timed out");
+    if (bits & DEV_ERR_INPUT) return fail(SLCS_ERR_INVALID, "a device-side input check failed (not a permutation)");
     if (bits) return fail(SLCS_ERR_DEVICE, "device status bits " + std::to_string(bits));
     return SLCS_OK;
 }
@@ -283,6 +305,7 @@ slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_
     L.counters = work;
     L.progress = work + 4;
     L.status = device_status_word();
+    L.wait_ns = wait_limit_ns(cfg);
     L.single.a_off = 0;
     L.single.b_off = 0;
     L.single.m = m;
@@ -370,13 +393,43 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
         std::nth_element(ms.begin(), ms.begin() + ms.size() / 2, ms.end());
         med = ms[ms.size() / 2];
     }
-    P->tm = pick_tile_m(cfg, med, cells);
     P->warps = pick_warps(cfg);
     P->use_graph = cfg && cfg->use_graph;
+    P->wait_ns = wait_limit_ns(cfg);
     P->npairs = npairs;
-    if (!tile_m_supported(P->tm)) {
-        delete P;
-        return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+    const bool wavefront_only = cfg && cfg->algo == SLCS_ALGO_WAVEFRONT;
+    if (wavefront_only) {
+        P->tm = pick_tile_m(cfg, med, cells);
+        if (!tile_m_supported(P->tm)) {
+            delete P;
+            return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+        }
+    } else {
+        // Stream mode: single-stripe pairs stream through segments; larger
+        // pairs run as wavefront tasks of BATCH_WF_TM rows per lane.
+        P->tm = BATCH_WF_TM;
+        P->seg = (cfg && cfg->seg) ? cfg->seg : 16;
+        if (cfg && cfg->tile_m) {
+            P->stm = cfg->tile_m;
+        } else {
+            // Fixed heuristic: the smallest rows-per-lane whose segment holds
+            // nine pairs in ten whole.
+            int32_t p90 = 0;
+            if (!ms.empty()) {
+                std::nth_element(ms.begin(), ms.begin() + (ms.size() * 9) / 10, ms.end());
+                p90 = ms[(ms.size() * 9) / 10];
+            }
+            P->stm = 16;
+            for (int t : {4, 8, 12, 16})
+                if (P->seg * t >= p90) {
+                    P->stm = t;
+                    break;
+                }
+        }
+        if (!stream_variant_supported(P->stm, P->seg)) {
+            delete P;
+            return fail(SLCS_ERR_UNSUPPORTED, "stream mode needs tile_m in {4,8,12,16} and seg in {8,16,32}");
+        }
     }
     for (int32_t p = 0; p < npairs; ++p) {
         if (pairs[p].m == 0 || pairs[p].n == 0) P->empty_pairs.push_back(pairs[p]);
@@ -384,14 +437,32 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
         P->need_b = std::max<int64_t>(P->need_b, pairs[p].b_offset + pairs[p].n);
         P->need_out = std::max<int64_t>(P->need_out, pairs[p].out_offset + pairs[p].m + pairs[p].n);
     }
-    Schedule S = build_schedule(pairs, npairs, P->tm);
+    Schedule S = build_schedule(pairs, npairs, P->tm, P->stm > 0 ? P->seg * P->stm : 0);
     P->ntasks = int32_t(S.tasks.size());
+    // One-time device set-up now, so a graph capture in run() issues only
+    // capturable work: the mapped status word and the occupancy queries.
+    device_status_word();
+    {
+        CombLaunch dummy{};
+        dummy.ntasks = 1;
+        slcs_status ps = P->stm > 0 ? launch_batch(BatchLaunch{dummy, nullptr, 1}, P->stm, P->seg, PREPARE_ONLY, nullptr)
+                                    : launch_comb(dummy, P->tm, P->warps, PREPARE_ONLY, nullptr);
+        if (ps != SLCS_OK) {
+            delete P;
+            return ps;
+        }
+    }
+    P->nstream = int32_t(S.stream_pairs.size());
     P->work_bytes = align_up(sizeof(int32_t) * (4 + S.tasks.size()), 256);
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void **ptr, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(ptr, bytes < 16 ? 16 : bytes);
     };
     alloc(reinterpret_cast<void **>(&P->d_pairs), sizeof(PairDev) * size_t(npairs));
+    alloc(reinterpret_cast<void **>(&P->d_stream), sizeof(int32_t) * S.stream_pairs.size());
+    if (e == cudaSuccess && !S.stream_pairs.empty())
+        e = cudaMemcpy(P->d_stream, S.stream_pairs.data(), sizeof(int32_t) * S.stream_pairs.size(),
+                       cudaMemcpyHostToDevice);
     alloc(reinterpret_cast<void **>(&P->d_tasks), sizeof(int2) * S.tasks.size());
     alloc(reinterpret_cast<void **>(&P->d_scr_off), sizeof(int64_t) * size_t(npairs));
     alloc(reinterpret_cast<void **>(&P->d_scratch), sizeof(int32_t) * size_t(S.scratch_elems) + 16);
@@ -410,10 +481,23 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
     return SLCS_OK;
 }
 
+slcs_status slcs_batch_plan_info(const slcs_batch_plan *P, slcs_plan_info *info)
+{
+    if (!P || !info) return fail(SLCS_ERR_INVALID, "null plan or info");
+    std::memset(info, 0, sizeof(*info));
+    info->stream_tile_m = P->stm;
+    info->seg = P->stm > 0 ? P->seg : 0;
+    info->wavefront_tile_m = P->tm;
+    info->warps = P->warps;
+    info->stream_pairs = P->nstream;
+    info->wavefront_tasks = P->ntasks;
+    return SLCS_OK;
+}
+
 int32_t slcs_batch_plan_launches(const slcs_batch_plan *P)
 {
     if (!P) return 0;
-    return (P->ntasks > 0 ? 1 : 0) + int32_t(P->empty_pairs.size());
+    return ((P->ntasks > 0 || P->nstream > 0) ? 1 : 0) + int32_t(P->empty_pairs.size());
 }
 
 slcs_status slcs_batch_plan_run(slcs_batch_plan *P, const uint8_t *a, const uint8_t *b, int32_t *out, void *stream)
@@ -487,6 +571,7 @@ slcs_status slcs_batch_plan_destroy(slcs_batch_plan *P)
     if (P->gexec) cudaGraphExecDestroy(P->gexec);
     if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
     cudaFree(P->d_pairs);
+    cudaFree(P->d_stream);
     cudaFree(P->d_tasks);
     cudaFree(P->d_scr_off);
     cudaFree(P->d_scratch);
@@ -574,10 +659,23 @@ int64_t slcs_permutation_hash(const int32_t *col_to_row, int32_t size)
     return r;
 }
 
-slcs_status slcs_braid_multiply(const int32_t *, int32_t, const int32_t *, int32_t, int32_t, int32_t, int32_t *,
-                                const slcs_config *, void *)
+slcs_status slcs_braid_multiply(const int32_t *p_r2c, int32_t p_size, const int32_t *q_r2c, int32_t q_size,
+                                int32_t k, int32_t row_glue, int32_t *out_r2c, const slcs_config *cfg, void *stream)
 {
-    return fail(SLCS_ERR_UNSUPPORTED, "braid multiplication is not built yet");
+    if (p_size < 0 || q_size < 0 || k < 0 || k > p_size || k > q_size)
+        return fail(SLCS_ERR_INVALID, "need 0 <= k <= min(p_size, q_size)");
+    if ((p_size && !p_r2c) || (q_size && !q_r2c) || (p_size + q_size - k > 0 && !out_r2c))
+        return fail(SLCS_ERR_INVALID, "null permutation pointer");
+    if (p_size + q_size == 0) return SLCS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    size_t bytes = 0;
+    braid_workspace_bytes(p_size, q_size, k, &bytes);
+    void *ws = nullptr;
+    SLCS_CUDA(cudaMallocAsync(&ws, bytes, st));
+    const int cutoff = (cfg && cfg->braid_cutoff > 0) ? cfg->braid_cutoff : 1024;
+    slcs_status s = launch_braid(p_r2c, p_size, q_r2c, q_size, k, row_glue != 0, out_r2c, cutoff, ws, bytes, st);
+    SLCS_CUDA(cudaFreeAsync(ws, st));
+    return s;
 }
 
 } // extern "C"

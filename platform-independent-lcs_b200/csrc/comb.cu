@@ -49,6 +49,7 @@ struct StripeWait {
     const int32_t *prog;
     int32_t *abort_flag;
     uint32_t *status;
+    uint64_t limit_ns;
     int32_t avail;
     uint64_t t0;
     bool dead;
@@ -67,7 +68,7 @@ struct StripeWait {
             uint64_t now = globaltimer_ns();
             if (t0 == 0) {
                 t0 = now;
-            } else if (now - t0 > WAIT_LIMIT_NS) {
+            } else if (now - t0 > limit_ns) {
                 dead = true;
                 st_relaxed_gpu(abort_flag, 1);
                 raise_status(status, DEV_ERR_TIMEOUT);
@@ -111,7 +112,7 @@ __device__ __forceinline__ void comb_stripe(const CombLaunch &L, const PairDev &
     const int nb = (n + TN - 1) / TN;
     const bool b_aligned = (reinterpret_cast<uintptr_t>(b) & 3) == 0;
 
-    StripeWait W{L.progress + (task - 1), L.counters + 1, L.status, 0, 0, false};
+    StripeWait W{L.progress + (task - 1), L.counters + 1, L.status, L.wait_ns, 0, 0, false};
     int32_t *prog_mine = L.progress + task;
 
     if (!first && lane == 0) {
@@ -241,6 +242,189 @@ __global__ void __launch_bounds__(WARPS * 32) comb_wavefront_kernel(const CombLa
     }
 }
 
+// ---------------------------------------------------------------------------
+// Stream mode (pairs of at most SEG*TM rows).
+//
+// A segment of SEG lanes is a SEG-deep systolic pipeline like the wavefront
+// warp, but its column stream is the concatenation of many pairs: lane l is
+// always l blocks behind lane 0, and when a lane finishes the last block of
+// one pair it writes its h strands, loads the next pair's symbols (fetched one
+// pair ahead) and carries on.  The pipeline fills and drains once per segment
+// instead of once per pair.  Segment lane 0 takes pairs from a global ticket
+// counter one pair ahead and publishes them in a shared-memory ring; the
+// other lanes read the ring when they reach that pair.
+// ---------------------------------------------------------------------------
+constexpr int SRING = 64; // ring slots per segment (> lanes a segment can lag)
+
+template <int TM>
+struct StreamTask {
+    int pair; // -1: no more work
+    int m, n, nb;
+    const uint8_t *b;
+    int32_t *h_out;
+    int32_t *v_out;
+};
+
+template <int TM>
+__device__ __forceinline__ void load_task(const CombLaunch &L, int pair, StreamTask<TM> &T)
+{
+    T.pair = pair;
+    if (pair < 0) {
+        T.m = T.n = T.nb = 0;
+        return;
+    }
+    const PairDev P = L.pairs[pair];
+    T.m = P.m;
+    T.n = P.n;
+    T.nb = (P.n + TN - 1) / TN;
+    T.b = L.b_blob + P.b_off;
+    T.h_out = L.out + P.out_off;
+    T.v_out = T.h_out + P.m;
+}
+
+// Rows [r0, r0+TM) of pair `pair`: symbols into av, start ids into hv.
+template <int TM>
+__device__ __forceinline__ void load_rows(const CombLaunch &L, int pair, int m, int r0, int (&av)[TM], int (&hv)[TM])
+{
+    if (pair < 0 || r0 >= m) {
+#pragma unroll
+        for (int k = 0; k < TM; ++k) {
+            av[k] = -1;
+            hv[k] = INT_MIN;
+        }
+        return;
+    }
+    const uint8_t *a = L.a_blob + L.pairs[pair].a_off + r0;
+    const bool full = r0 + TM <= m;
+    if (full && (TM % 4 == 0) && (reinterpret_cast<uintptr_t>(a) & 3) == 0) {
+#pragma unroll
+        for (int q = 0; q < TM / 4; ++q) {
+            const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(a) + q);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) av[4 * q + k] = int((w >> (8 * k)) & 0xffu);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < TM; ++k) av[k] = (r0 + k < m) ? int(__ldg(a + k)) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < TM; ++k) hv[k] = (r0 + k < m) ? (m - 1 - r0 - k) : INT_MIN;
+}
+
+template <int TM, int SEG>
+__device__ __forceinline__ void stream_segment(const BatchLaunch &B, int *ring, int lane)
+{
+    const CombLaunch &L = B.wf;
+    const int sl = lane & (SEG - 1); // lane within the segment
+    int *ticket = L.counters + 2;
+
+    // Segment lane 0 publishes the first two pairs before anyone starts.
+    int next_ticket = 0;
+    if (sl == 0) {
+        const int t0 = atomicAdd(ticket, 1);
+        ring[0] = t0 < B.nstream ? B.stream_pairs[t0] : -1;
+        next_ticket = atomicAdd(ticket, 1);
+    }
+    __syncwarp();
+
+    int q = 0; // index of this lane's current pair within the segment's stream
+    StreamTask<TM> T;
+    load_task<TM>(L, ring[0], T);
+    int av[TM], hv[TM];
+    load_rows<TM>(L, T.pair, T.m, sl * TM, av, hv);
+    int blk = -sl;
+
+    int vc[TN];
+#pragma unroll
+    for (int j = 0; j < TN; ++j) vc[j] = INT_MAX;
+
+    for (;;) {
+        const bool busy = T.pair >= 0;
+        if (!__any_sync(FULL_MASK, busy)) break;
+        const bool act = busy && blk >= 0;
+
+        int vi[TN];
+#pragma unroll
+        for (int j = 0; j < TN; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1, SEG);
+        if (sl == 0) {
+            const int c = blk * TN;
+#pragma unroll
+            for (int j = 0; j < TN; ++j) vi[j] = (act && c + j < T.n) ? T.m + c + j : INT_MAX;
+        }
+
+        int bs[TN];
+        if (act) {
+            const int c = blk * TN;
+            if (c + TN <= T.n && (reinterpret_cast<uintptr_t>(T.b) & 3) == 0) {
+                const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(T.b + c));
+#pragma unroll
+                for (int j = 0; j < TN; ++j) bs[j] = int((w >> (8 * j)) & 0xffu);
+            } else {
+#pragma unroll
+                for (int j = 0; j < TN; ++j) bs[j] = (c + j < T.n) ? int(__ldg(T.b + c + j)) : -2;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < TN; ++j) bs[j] = -2;
+        }
+
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+            int v = vi[j];
+#pragma unroll
+            for (int k = 0; k < TM; ++k) cell(av[k], bs[j], hv[k], v);
+            vc[j] = v;
+        }
+
+        if (sl == SEG - 1 && act) {
+            const int c = blk * TN;
+#pragma unroll
+            for (int j = 0; j < TN; ++j)
+                if (c + j < T.n) T.v_out[c + j] = vc[j];
+        }
+
+        if (busy && ++blk == T.nb) {
+            // This lane leaves pair q: write its h strands, move to pair q+1.
+            const int r0 = sl * TM;
+#pragma unroll
+            for (int k = 0; k < TM; ++k)
+                if (r0 + k < T.m) T.h_out[T.m - 1 - r0 - k] = hv[k];
+            ++q;
+            if (sl == 0) {
+                ring[q & (SRING - 1)] = next_ticket < B.nstream ? B.stream_pairs[next_ticket] : -1;
+                next_ticket = next_ticket < B.nstream ? atomicAdd(ticket, 1) : next_ticket;
+            }
+            // Lane 0 wrote slot q in an earlier step (or just now for itself).
+            const int pair = ring[q & (SRING - 1)];
+            load_task<TM>(L, pair, T);
+            load_rows<TM>(L, T.pair, T.m, r0, av, hv);
+            blk = 0;
+        }
+        __syncwarp();
+    }
+}
+
+template <int TM, int SEG, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) comb_batch_kernel(const BatchLaunch B)
+{
+    __shared__ __align__(16) int4 wf_ring[WARPS][RING];
+    __shared__ int s_ring[WARPS][32 / SEG][SRING];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const CombLaunch &L = B.wf;
+    // Phase 1: stripes of multi-stripe pairs, whole warps, wavefront order.
+    for (;;) {
+        int k = 0;
+        if (lane == 0) k = ld_relaxed_gpu(L.counters + 1) ? INT_MAX : atomicAdd(L.counters, 1);
+        k = __shfl_sync(FULL_MASK, k, 0);
+        if (k >= L.ntasks) break;
+        const int2 tk = L.tasks[k];
+        comb_stripe<BATCH_WF_TM>(L, L.pairs[tk.x], L.scratch_off[tk.x], tk.y, k, wf_ring[w], lane);
+    }
+    // Phase 2: single-stripe pairs streamed through segments.
+    if (B.nstream > 0) stream_segment<TM, SEG>(B, s_ring[w][lane / SEG], lane);
+}
+
 __global__ void strands_to_perm_kernel(const int32_t *__restrict__ h, int32_t m, const int32_t *__restrict__ v,
                                        int32_t n, int32_t *r2c, int32_t *c2r)
 {
@@ -268,6 +452,7 @@ slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_o
             if (occ < 1) occ = 1;
         }
     }
+    if (stream == PREPARE_ONLY) return SLCS_OK;
     const long want = (long(L.ntasks) + WARPS - 1) / WARPS;
     long grid = long(sm_count()) * occ;
     if (want < grid) grid = want;
@@ -278,7 +463,58 @@ slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_o
     return SLCS_OK;
 }
 
+template <int TM, int SEG, int WARPS>
+slcs_status launch_batch_variant(const BatchLaunch &B, cudaStream_t stream, int *grid_out)
+{
+    static int occ = -1;
+    static std::mutex mu;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (occ < 0) {
+            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_batch_kernel<TM, SEG, WARPS>,
+                                                                    WARPS * 32, 0));
+            if (occ < 1) occ = 1;
+        }
+    }
+    if (stream == PREPARE_ONLY) return SLCS_OK;
+    const long segs_per_block = long(WARPS) * (32 / SEG);
+    long want = (long(B.nstream) + segs_per_block - 1) / segs_per_block;
+    const long want_wf = (long(B.wf.ntasks) + WARPS - 1) / WARPS;
+    if (want_wf > want) want = want_wf;
+    long grid = long(sm_count()) * occ;
+    if (want < grid) grid = want;
+    if (grid < 1) grid = 1;
+    comb_batch_kernel<TM, SEG, WARPS><<<int(grid), WARPS * 32, 0, stream>>>(B);
+    if (grid_out) *grid_out = int(grid);
+    SLCS_CUDA(cudaGetLastError());
+    return SLCS_OK;
+}
+
 } // namespace
+
+bool stream_variant_supported(int tm, int seg)
+{
+    return (tm == 4 || tm == 8 || tm == 12 || tm == 16) && (seg == 8 || seg == 16 || seg == 32);
+}
+
+slcs_status launch_batch(const BatchLaunch &B, int tm, int seg, cudaStream_t stream, int *grid_out)
+{
+    if (B.wf.ntasks <= 0 && B.nstream <= 0) return SLCS_OK;
+#define SLCS_SEG_CASE(TM)                                                               \
+    case TM:                                                                            \
+        if (seg == 8) return launch_batch_variant<TM, 8, 4>(B, stream, grid_out);       \
+        if (seg == 16) return launch_batch_variant<TM, 16, 4>(B, stream, grid_out);     \
+        return launch_batch_variant<TM, 32, 4>(B, stream, grid_out);
+    if (!stream_variant_supported(tm, seg)) return fail(SLCS_ERR_UNSUPPORTED, "stream tile_m/seg not supported");
+    switch (tm) {
+        SLCS_SEG_CASE(4)
+        SLCS_SEG_CASE(8)
+        SLCS_SEG_CASE(12)
+        SLCS_SEG_CASE(16)
+    }
+#undef SLCS_SEG_CASE
+    return fail(SLCS_ERR_UNSUPPORTED, "stream tile_m/seg not supported");
+}
 
 bool tile_m_supported(int tm) { return tm == 2 || tm == 4 || tm == 8 || tm == 12 || tm == 16; }
 int rows_per_stripe(int tm) { return 32 * tm; }

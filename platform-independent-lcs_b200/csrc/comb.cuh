@@ -21,7 +21,18 @@ struct CombLaunch {
     int32_t *progress;          // ntasks counters (blocks of 4 columns published)
     int32_t *counters;          // [0] ticket, [1] abort flag
     uint32_t *status;           // mapped device status word
+    uint64_t wait_ns;           // limit of one bounded wait
     PairDev single;
+};
+
+// A batch launch: multi-stripe pairs go through the wavefront tasks above
+// (whole warps, tile_m rows per lane), then every single-stripe pair is
+// streamed: a segment of `seg` lanes combs pair after pair without draining
+// its pipeline between them.
+struct BatchLaunch {
+    CombLaunch wf;              // wavefront part (tasks of multi-stripe pairs)
+    const int32_t *stream_pairs; // device: single-stripe pairs, largest first
+    int32_t nstream;
 };
 
 // Rows of a one lane keeps in registers; supported values.
@@ -35,8 +46,19 @@ inline int64_t scratch_elems(int32_t m, int32_t n, int tm)
     return stripes_of(m, tm) > 1 ? (int64_t(n) + 3) / 4 * 4 : 0;
 }
 
+// Passed as the stream, makes a launch function only do its one-time set-up
+// (occupancy query), so that a later launch can be captured into a graph.
+static const cudaStream_t PREPARE_ONLY = reinterpret_cast<cudaStream_t>(~uintptr_t(0));
+
 // Enqueue one persistent launch; `counters` and `progress` must be zero.
 slcs_status launch_comb(const CombLaunch &L, int tile_m, int warps, cudaStream_t stream, int *grid_out);
+
+// Stream-mode variants: rows per lane and lanes per segment.
+bool stream_variant_supported(int stream_tm, int seg);
+// Enqueue one persistent batch launch (counters [0] wavefront ticket, [1]
+// abort, [2] stream ticket must be zero).  Wavefront tasks use tile_m 8.
+slcs_status launch_batch(const BatchLaunch &L, int stream_tm, int seg, cudaStream_t stream, int *grid_out);
+constexpr int BATCH_WF_TM = 8;
 
 // Strands -> permutation matrix arrays (either output may be null).
 slcs_status launch_strands_to_perm(const int32_t *h, int32_t m, const int32_t *v, int32_t n,

@@ -16,10 +16,16 @@ constexpr unsigned FULL_MASK = 0xffffffffu;
 enum : uint32_t {
     DEV_ERR_TIMEOUT = 1u << 0, // a bounded wait on another warp's progress expired
     DEV_ERR_BOUNDS = 1u << 1,  // an index check failed (checked builds)
+    DEV_ERR_INPUT = 1u << 2,   // a device-side input check failed (e.g. not a permutation)
 };
 
-// A bounded wait gives up after this many nanoseconds of %globaltimer.
-constexpr uint64_t WAIT_LIMIT_NS = 4000000000ull;
+// A bounded wait gives up after this many nanoseconds of %globaltimer unless
+// the configuration sets another limit (slcs_config::wait_ms).
+constexpr uint64_t DEFAULT_WAIT_NS = 10000000000ull;
+inline uint64_t wait_limit_ns(const slcs_config *cfg)
+{
+    return (cfg && cfg->wait_ms > 0) ? uint64_t(cfg->wait_ms) * 1000000ull : DEFAULT_WAIT_NS;
+}
 
 // One pair of a launch: identical layout to slcs_pair_desc.
 struct PairDev {

@@ -29,7 +29,8 @@ class SlcsError(RuntimeError):
 class Config(ctypes.Structure):
     _fields_ = [("algo", ctypes.c_int32), ("tile_m", ctypes.c_int32), ("tile_n", ctypes.c_int32),
                 ("warps", ctypes.c_int32), ("braid_cutoff", ctypes.c_int32), ("strips", ctypes.c_int32),
-                ("use_graph", ctypes.c_int32), ("reserved", ctypes.c_int32 * 9)]
+                ("use_graph", ctypes.c_int32), ("seg", ctypes.c_int32), ("wait_ms", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 7)]
 
     @classmethod
     def make(cls, **kw) -> "Config":
@@ -43,6 +44,15 @@ class Config(ctypes.Structure):
 class PairDesc(ctypes.Structure):
     _fields_ = [("a_offset", ctypes.c_int64), ("b_offset", ctypes.c_int64), ("out_offset", ctypes.c_int64),
                 ("m", ctypes.c_int32), ("n", ctypes.c_int32)]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("stream_tile_m", ctypes.c_int32), ("seg", ctypes.c_int32), ("wavefront_tile_m", ctypes.c_int32),
+                ("warps", ctypes.c_int32), ("stream_pairs", ctypes.c_int32), ("wavefront_tasks", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 2)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
 
 
 PAIR_DTYPE = np.dtype([("a_offset", np.int64), ("b_offset", np.int64), ("out_offset", np.int64),
@@ -77,6 +87,7 @@ def lib():
         L.slcs_batch_plan_run_host.argtypes = [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp]
         L.slcs_batch_plan_launches.argtypes = [_vp]
         L.slcs_batch_plan_launches.restype = _i32
+        L.slcs_batch_plan_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
         L.slcs_strands_to_permutation.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, _vp]
         L.slcs_permutation_hash.argtypes = [_vp, _i32]
         L.slcs_permutation_hash.restype = _i64
@@ -165,6 +176,12 @@ class BatchPlan:
     @property
     def launches(self) -> int:
         return int(lib().slcs_batch_plan_launches(self._h))
+
+    @property
+    def info(self) -> dict:
+        pi = PlanInfo()
+        check(lib().slcs_batch_plan_info(self._h, ctypes.byref(pi)))
+        return pi.as_dict()
 
     def run(self, a_blob, b_blob, out, stream=None):
         check(lib().slcs_batch_plan_run(self._h, _dptr(a_blob), _dptr(b_blob), _dptr(out), _stream(stream)))

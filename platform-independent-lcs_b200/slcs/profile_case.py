@@ -1,0 +1,52 @@
+"""Small, self-contained launches for ncu captures.
+
+    python -m slcs.profile_case batch [npairs]     # one batch launch (read/window pairs)
+    python -m slcs.profile_case pair  [length]     # one square uniform pair
+
+Each case runs one warm-up launch and then the launch to capture, and checks
+the device status word; it holds a few hundred MB on the device at most.
+"""
+import sys
+
+import numpy as np
+import torch
+
+import slcs
+from slcs import workloads as W
+
+
+def main():
+    kind = sys.argv[1] if len(sys.argv) > 1 else "batch"
+    size = int(sys.argv[2]) if len(sys.argv) > 2 else 0
+    tm = int(sys.argv[3]) if len(sys.argv) > 3 else 0
+    dev = torch.device("cuda:0")
+    if kind == "batch":
+        batch = W.reads_20000(npairs=size or 20000)
+        _, total = batch.strand_offsets()
+        cfg = slcs.Config.make(tile_m=tm or 8)
+        plan = slcs.BatchPlan(slcs.pair_descs(batch), cfg)
+        a = torch.from_numpy(batch.a_blob).to(dev)
+        b = torch.from_numpy(batch.b_blob).to(dev)
+        out = torch.empty(total, dtype=torch.int32, device=dev)
+        for _ in range(2):
+            plan.run(a, b, out)
+        torch.cuda.synchronize()
+        plan.close()
+    elif kind == "pair":
+        n = size or 65536
+        rng = np.random.default_rng(1)
+        a = torch.from_numpy(rng.integers(0, 4, n, dtype=np.uint8)).to(dev)
+        b = torch.from_numpy(rng.integers(0, 4, n, dtype=np.uint8)).to(dev)
+        out = torch.empty(2 * n, dtype=torch.int32, device=dev)
+        cfg = slcs.Config.make(tile_m=tm or 16)
+        for _ in range(2):
+            slcs.comb_pair(a, b, cfg=cfg, out=out)
+        torch.cuda.synchronize()
+    else:
+        raise SystemExit(f"unknown case {kind}")
+    slcs.device_status(0)
+    print(f"profile case {kind} {size} done")
+
+
+if __name__ == "__main__":
+    main()

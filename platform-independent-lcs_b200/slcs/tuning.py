@@ -18,14 +18,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def heuristic_batch_config(batch) -> Config:
-    """Fixed rule: enough rows per lane that the median pair fits one stripe."""
-    med = int(np.median(batch.ms)) if batch.npairs else 0
-    tm = 2
-    for t in (2, 4, 8, 12, 16):
-        tm = t
-        if 32 * t >= med:
-            break
-    return Config.make(tile_m=tm, warps=4, use_graph=1)
+    """The library's fixed rule (stream mode, 16-lane segments, the smallest
+    rows-per-lane whose segment holds nine pairs in ten whole)."""
+    return Config.make(use_graph=1)
 
 
 def choose_batch_config(batch):

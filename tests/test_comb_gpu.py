@@ -126,21 +126,62 @@ def test_batch_reads(cuda, graph):
         np.testing.assert_array_equal(out.cpu().numpy(), want)
 
 
-def test_batch_mixed_sizes(cuda):
-    import torch
-    rng = np.random.default_rng(11)
+def _mixed_batch(seed, count=300, mmax=1500, nmax=1500):
+    rng = np.random.default_rng(seed)
     pairs = []
-    for _ in range(300):
-        m = int(rng.integers(0, 1500)); n = int(rng.integers(0, 1500))
+    for _ in range(count):
+        m = int(rng.integers(0, mmax)); n = int(rng.integers(0, nmax))
         sigma = int(rng.choice([2, 4, 256]))
         pairs.append((rng.integers(0, sigma, m, dtype=np.uint8), rng.integers(0, sigma, n, dtype=np.uint8)))
+    return W.pack(pairs)
+
+
+def test_batch_mixed_sizes_wavefront(cuda):
+    import torch
+    batch = _mixed_batch(11)
+    descs = slcs.pair_descs(batch)
+    _, total = batch.strand_offsets()
+    want = _batch_expected(batch)
+    for tm in (2, 8, 16):
+        out = torch.full((total,), -7, dtype=torch.int32, device=cuda)
+        slcs.comb_batch(descs, _dev(batch.a_blob, cuda), _dev(batch.b_blob, cuda), out,
+                        slcs.Config.make(algo=slcs.ALGO_WAVEFRONT, tile_m=tm))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy(), want)
+    host = slcs.comb_batch_host(descs, batch.a_blob, batch.b_blob, total)
+    np.testing.assert_array_equal(host, want)
+
+
+@pytest.mark.parametrize("stm,seg", [(4, 8), (4, 32), (8, 16), (12, 16), (16, 8), (16, 16), (16, 32)])
+def test_batch_stream_variants(cuda, stm, seg):
+    """Stream mode (pairs of at most seg*stm rows) plus wavefront tasks for the rest."""
+    import torch
+    batch = _mixed_batch(20 + stm + seg, count=400, mmax=700, nmax=900)
+    descs = slcs.pair_descs(batch)
+    _, total = batch.strand_offsets()
+    want = _batch_expected(batch)
+    plan = slcs.BatchPlan(descs, slcs.Config.make(tile_m=stm, seg=seg))
+    info = plan.info
+    assert info["stream_tile_m"] == stm and info["seg"] == seg and info["stream_pairs"] > 0
+    out = torch.full((total,), -7, dtype=torch.int32, device=cuda)
+    plan.run(_dev(batch.a_blob, cuda), _dev(batch.b_blob, cuda), out)
+    torch.cuda.synchronize()
+    slcs.device_status(0)
+    np.testing.assert_array_equal(out.cpu().numpy(), want)
+
+
+def test_batch_stream_tiny_pairs(cuda):
+    """Pairs of one block or less: the segment switches pairs every step."""
+    import torch
+    rng = np.random.default_rng(99)
+    pairs = [(rng.integers(0, 3, int(rng.integers(1, 9)), dtype=np.uint8),
+              rng.integers(0, 3, int(rng.integers(1, 6)), dtype=np.uint8)) for _ in range(500)]
     batch = W.pack(pairs)
     descs = slcs.pair_descs(batch)
     _, total = batch.strand_offsets()
-    for tm in (2, 8, 16):
+    for seg in (8, 16, 32):
         out = torch.full((total,), -7, dtype=torch.int32, device=cuda)
-        slcs.comb_batch(descs, _dev(batch.a_blob, cuda), _dev(batch.b_blob, cuda), out, slcs.Config.make(tile_m=tm))
+        plan = slcs.BatchPlan(descs, slcs.Config.make(tile_m=4, seg=seg))
+        plan.run(_dev(batch.a_blob, cuda), _dev(batch.b_blob, cuda), out)
         torch.cuda.synchronize()
         np.testing.assert_array_equal(out.cpu().numpy(), _batch_expected(batch))
-    host = slcs.comb_batch_host(descs, batch.a_blob, batch.b_blob, total)
-    np.testing.assert_array_equal(host, _batch_expected(batch))
