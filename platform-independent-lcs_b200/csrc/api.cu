@@ -7,6 +7,7 @@
 #include <cstring>
 #include <mutex>
 #include <numeric>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -163,10 +164,13 @@ struct slcs_batch_plan {
     int32_t npairs = 0;
     int32_t ntasks = 0;
     int32_t nstream = 0;
+    int32_t nseg = 0;   // stream segments with a pair list
+    int grid = 0;       // blocks of the batch launch
     uint64_t wait_ns = DEFAULT_WAIT_NS;
     bool use_graph = false;
     PairDev *d_pairs = nullptr;
-    int32_t *d_stream = nullptr;
+    int32_t *d_seg_off = nullptr;
+    int32_t *d_seg_list = nullptr;
     int2 *d_tasks = nullptr;
     int64_t *d_scr_off = nullptr;
     int32_t *d_scratch = nullptr;
@@ -205,7 +209,7 @@ struct slcs_batch_plan {
         SLCS_CUDA(cudaMemsetAsync(d_work, 0, work_bytes, st));
         slcs_status s;
         if (stm > 0) {
-            BatchLaunch B{launch(a, b, out), d_stream, nstream};
+            BatchLaunch B{launch(a, b, out), d_seg_off, d_seg_list, nseg, grid};
             s = launch_batch(B, stm, seg, st, nullptr);
         } else {
             s = launch_comb(launch(a, b, out), tm, warps, st, nullptr);
@@ -442,10 +446,12 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
     // One-time device set-up now, so a graph capture in run() issues only
     // capturable work: the mapped status word and the occupancy queries.
     device_status_word();
+    int full_grid = 0;
     {
         CombLaunch dummy{};
         dummy.ntasks = 1;
-        slcs_status ps = P->stm > 0 ? launch_batch(BatchLaunch{dummy, nullptr, 1}, P->stm, P->seg, PREPARE_ONLY, nullptr)
+        slcs_status ps = P->stm > 0 ? launch_batch(BatchLaunch{dummy, nullptr, nullptr, 0, 0}, P->stm, P->seg,
+                                                   PREPARE_ONLY, &full_grid)
                                     : launch_comb(dummy, P->tm, P->warps, PREPARE_ONLY, nullptr);
         if (ps != SLCS_OK) {
             delete P;
@@ -453,16 +459,51 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
         }
     }
     P->nstream = int32_t(S.stream_pairs.size());
+    // Stream segments and their pair lists: longest processing time first
+    // (a pair costs its column blocks plus the switch), each pair to the least
+    // loaded segment; the grid is the persistent one, or fewer blocks when the
+    // batch is small.
+    std::vector<int32_t> seg_off, seg_list;
+    if (P->stm > 0) {
+        const int segs_per_block = BATCH_WARPS * (32 / P->seg);
+        int grid = std::max(1, full_grid);
+        const long want_stream = (long(P->nstream) + segs_per_block - 1) / segs_per_block;
+        const long want_wf = (long(P->ntasks) + BATCH_WARPS - 1) / BATCH_WARPS;
+        grid = int(std::min<long>(grid, std::max<long>(1, std::max(want_stream, want_wf))));
+        P->grid = grid;
+        P->nseg = P->nstream > 0 ? int32_t(std::min<long>(long(grid) * segs_per_block, P->nstream)) : 0;
+        if (P->nseg > 0) {
+            std::vector<std::vector<int32_t>> lists(P->nseg);
+            using Load = std::pair<int64_t, int32_t>;
+            std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+            for (int32_t sgi = 0; sgi < P->nseg; ++sgi) heap.push({0, sgi});
+            for (int32_t p : S.stream_pairs) { // already largest first
+                Load top = heap.top();
+                heap.pop();
+                lists[top.second].push_back(p);
+                top.first += (pairs[p].n + 3) / 4 + 2;
+                heap.push(top);
+            }
+            seg_off.reserve(P->nseg + 1);
+            seg_off.push_back(0);
+            for (auto &l : lists) {
+                seg_list.insert(seg_list.end(), l.begin(), l.end());
+                seg_off.push_back(int32_t(seg_list.size()));
+            }
+        }
+    }
     P->work_bytes = align_up(sizeof(int32_t) * (4 + S.tasks.size()), 256);
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void **ptr, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(ptr, bytes < 16 ? 16 : bytes);
     };
     alloc(reinterpret_cast<void **>(&P->d_pairs), sizeof(PairDev) * size_t(npairs));
-    alloc(reinterpret_cast<void **>(&P->d_stream), sizeof(int32_t) * S.stream_pairs.size());
-    if (e == cudaSuccess && !S.stream_pairs.empty())
-        e = cudaMemcpy(P->d_stream, S.stream_pairs.data(), sizeof(int32_t) * S.stream_pairs.size(),
-                       cudaMemcpyHostToDevice);
+    alloc(reinterpret_cast<void **>(&P->d_seg_off), sizeof(int32_t) * seg_off.size());
+    alloc(reinterpret_cast<void **>(&P->d_seg_list), sizeof(int32_t) * seg_list.size());
+    if (e == cudaSuccess && !seg_off.empty())
+        e = cudaMemcpy(P->d_seg_off, seg_off.data(), sizeof(int32_t) * seg_off.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !seg_list.empty())
+        e = cudaMemcpy(P->d_seg_list, seg_list.data(), sizeof(int32_t) * seg_list.size(), cudaMemcpyHostToDevice);
     alloc(reinterpret_cast<void **>(&P->d_tasks), sizeof(int2) * S.tasks.size());
     alloc(reinterpret_cast<void **>(&P->d_scr_off), sizeof(int64_t) * size_t(npairs));
     alloc(reinterpret_cast<void **>(&P->d_scratch), sizeof(int32_t) * size_t(S.scratch_elems) + 16);
@@ -571,7 +612,8 @@ slcs_status slcs_batch_plan_destroy(slcs_batch_plan *P)
     if (P->gexec) cudaGraphExecDestroy(P->gexec);
     if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
     cudaFree(P->d_pairs);
-    cudaFree(P->d_stream);
+    cudaFree(P->d_seg_off);
+    cudaFree(P->d_seg_list);
     cudaFree(P->d_tasks);
     cudaFree(P->d_scr_off);
     cudaFree(P->d_scratch);
@@ -668,11 +710,11 @@ slcs_status slcs_braid_multiply(const int32_t *p_r2c, int32_t p_size, const int3
         return fail(SLCS_ERR_INVALID, "null permutation pointer");
     if (p_size + q_size == 0) return SLCS_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int cutoff = (cfg && cfg->braid_cutoff > 0) ? cfg->braid_cutoff : 1024;
     size_t bytes = 0;
-    braid_workspace_bytes(p_size, q_size, k, &bytes);
+    braid_workspace_bytes(p_size, q_size, k, cutoff, &bytes);
     void *ws = nullptr;
     SLCS_CUDA(cudaMallocAsync(&ws, bytes, st));
-    const int cutoff = (cfg && cfg->braid_cutoff > 0) ? cfg->braid_cutoff : 1024;
     slcs_status s = launch_braid(p_r2c, p_size, q_r2c, q_size, k, row_glue != 0, out_r2c, cutoff, ws, bytes, st);
     SLCS_CUDA(cudaFreeAsync(ws, st));
     return s;

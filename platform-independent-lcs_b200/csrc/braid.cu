@@ -578,6 +578,253 @@ __global__ void __launch_bounds__(128) walk_seq_kernel(GlueArgs A)
 }
 
 // ---------------------------------------------------------------------------
+// concurrent walk of large nodes
+//
+// delta(r, c) = #{hi points with row < r, col < c} - #{lo points with row >= r,
+// col >= c} is non-decreasing in r and in c, changes by 0 or 1 per unit step,
+// and the reference's walk turns right where it is negative and up where it
+// is zero.  Each step moves to the next diagonal e = col - row, and the walk's
+// row on diagonal e is r*(e-1) - 1 with r*(e) the first row of diagonal e whose
+// delta is >= 0.  A level therefore tabulates delta at the grid points that
+// are multiples of B (per node, a (G+1)^2 table from block counts), and walk
+// segment q, which owns diagonals (E, E+B] for E a multiple of B, finds r*(E)
+// by a binary search over the table and a warp scan inside one block, then
+// walks its B diagonals alone.  Every segment writes its fresh points.
+// ---------------------------------------------------------------------------
+constexpr int WALK_GMAX = 1024; // grid lines per node and dimension, at most
+constexpr int WALK_BMIN = 64;   // smallest grid spacing
+
+struct TableArgs {
+    const int32_t *C;
+    const uint8_t *H;
+    int32_t *cnt_hi; // (G+1)^2 per node, becomes the delta table
+    int32_t *cnt_lo;
+    int k, level, B, stride; // stride = Gmax+1 for the level
+    const int32_t *bad;
+};
+
+__device__ __forceinline__ void node_by_index(int nd, int level, int k, int &o, int &s)
+{
+    o = 0;
+    s = k;
+    for (int e = 0; e < level; ++e) {
+        const int h = s >> 1;
+        if ((nd >> (level - 1 - e)) & 1) {
+            o += h;
+            s -= h;
+        } else {
+            s = h;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) table_count_kernel(TableArgs A)
+{
+    if (*A.bad) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.k; i += gridDim.x * blockDim.x) {
+        // node and its index (the path of hi/lo choices)
+        int o = 0, s = A.k, nd = 0;
+        for (int d = 0; d < A.level; ++d) {
+            const int h = s >> 1;
+            nd <<= 1;
+            if (i < o + h) {
+                s = h;
+            } else {
+                o += h;
+                s -= h;
+                nd |= 1;
+            }
+        }
+        const int G = s / A.B;
+        const int bi = min((i - o) / A.B, G), bj = min(A.C[i] / A.B, G);
+        int32_t *t = (A.H[i] ? A.cnt_hi : A.cnt_lo) + size_t(nd) * A.stride * A.stride;
+        atomicAdd(t + bi * A.stride + bj, 1);
+    }
+}
+
+// Per (node, row block): exclusive prefix of hi counts and inclusive suffix of
+// lo counts along the columns.
+__global__ void __launch_bounds__(256) table_rows_kernel(TableArgs A, int nodes)
+{
+    if (*A.bad) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nodes * A.stride) return;
+    const int nd = t / A.stride, bi = t % A.stride;
+    int o, s;
+    node_by_index(nd, A.level, A.k, o, s);
+    const int G = s / A.B;
+    if (bi > G) return;
+    int32_t *hi = A.cnt_hi + size_t(nd) * A.stride * A.stride + size_t(bi) * A.stride;
+    int32_t *lo = A.cnt_lo + size_t(nd) * A.stride * A.stride + size_t(bi) * A.stride;
+    int run = 0;
+    for (int j = 0; j <= G; ++j) {
+        const int v = hi[j];
+        hi[j] = run;
+        run += v;
+    }
+    run = 0;
+    for (int j = G; j >= 0; --j) {
+        run += lo[j];
+        lo[j] = run;
+    }
+}
+
+// Per (node, grid column): finish the 2D sums and store the delta table.
+__global__ void __launch_bounds__(256) table_cols_kernel(TableArgs A, int nodes)
+{
+    if (*A.bad) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nodes * A.stride) return;
+    const int nd = t / A.stride, j = t % A.stride;
+    int o, s;
+    node_by_index(nd, A.level, A.k, o, s);
+    const int G = s / A.B;
+    if (j > G) return;
+    int32_t *hi = A.cnt_hi + size_t(nd) * A.stride * A.stride + j;
+    int32_t *lo = A.cnt_lo + size_t(nd) * A.stride * A.stride + j;
+    int run = 0;
+    for (int i = G; i >= 0; --i) {
+        run += lo[size_t(i) * A.stride];
+        lo[size_t(i) * A.stride] = run; // lo[i][j] = #lo points with row >= iB, col >= jB
+    }
+    run = 0;
+    for (int i = 0; i <= G; ++i) {
+        const int v = hi[size_t(i) * A.stride];
+        hi[size_t(i) * A.stride] = run - lo[size_t(i) * A.stride]; // delta(iB, jB)
+        run += v;
+    }
+}
+
+struct SegArgs {
+    const int32_t *C;
+    const uint8_t *H;
+    const int32_t *R;
+    const uint8_t *HC;
+    const int32_t *T; // delta tables
+    int32_t *res;
+    int k, level, B, stride, nseg; // nseg: segments per node
+    const int32_t *bad;
+};
+
+// delta(r+1, c) - delta(r, c): the point of row r joins the hi count or
+// leaves the lo count.
+__device__ __forceinline__ int rowinc(const SegArgs &A, int o, int r, int c)
+{
+    const int cc = A.C[o + r];
+    return A.H[o + r] ? (cc < c) : (cc >= c);
+}
+// delta(r, c+1) - delta(r, c)
+__device__ __forceinline__ int colinc(const SegArgs &A, int o, int c, int r)
+{
+    const int rr = A.R[o + c];
+    return A.HC[o + c] ? (rr < r) : (rr >= r);
+}
+
+__device__ __forceinline__ int warp_sum(int v)
+{
+    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(FULL_MASK, v, off);
+    return v;
+}
+
+// Exact delta(r, c) (0 <= r, c <= s): table value at the grid point below-left
+// plus the steps down column c0 and along row r, summed by the warp.
+__device__ int delta_at(const SegArgs &A, const int32_t *T, int o, int r, int c, int lane)
+{
+    const int i0 = r / A.B, j0 = c / A.B;
+    const int r0 = i0 * A.B, c0 = j0 * A.B;
+    int acc = 0;
+    for (int rr = r0 + lane; rr < r; rr += 32) acc += rowinc(A, o, rr, c0);
+    for (int cc = c0 + lane; cc < c; cc += 32) acc += colinc(A, o, cc, r);
+    return T[i0 * A.stride + j0] + warp_sum(acc);
+}
+
+__global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes)
+{
+    if (*A.bad) return;
+    const int lane = threadIdx.x & 31;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= nodes * A.nseg) return;
+    const int nd = w / A.nseg, q = w % A.nseg;
+    int o, s;
+    node_by_index(nd, A.level, A.k, o, s);
+    if (s <= 1) return;
+    const int B = A.B;
+    const int G = s / B;
+    const int32_t *T = A.T + size_t(nd) * A.stride * A.stride;
+    const int jmin = -((s + B - 1) / B); // floor(-s / B)
+    const int E = (jmin + q) * B;
+    const int e0 = -(s - 1);
+    if (E > s || E + B < e0) return;
+    int dr, dc, delta;
+    if (E < e0) {
+        dr = s - 1;
+        dc = 0;
+        delta = A.H[o + s - 1] ? 0 : -1;
+    } else {
+        const int rlo = max(0, -E), rhi = min(s, s - E);
+        if (rlo > rhi) return;
+        const int jj = E / B;
+        const int ilo = rlo / B, ihi = rhi / B;
+        // first grid point of diagonal E with delta >= 0
+        int lo_i = ilo, hi_i = ihi + 1;
+        while (lo_i < hi_i) {
+            const int mid = (lo_i + hi_i) >> 1;
+            if (T[mid * A.stride + mid + jj] >= 0) hi_i = mid;
+            else lo_i = mid + 1;
+        }
+        const int istar = lo_i;
+        int rstar;
+        if (istar == ilo) {
+            rstar = rlo;
+        } else {
+            int rb = (istar - 1) * B;
+            int dval = T[(istar - 1) * A.stride + (istar - 1) + jj];
+            const int rend = min(istar * B, rhi);
+            rstar = rhi + 1;
+            for (; rb < rend; rb += 32) {
+                const int r = rb + lane;
+                int inc = 0;
+                if (r < rend) inc = colinc(A, o, r + E, r) + rowinc(A, o, r, r + E + 1);
+                int pre = inc;
+                for (int off = 1; off < 32; off <<= 1) {
+                    const int y = __shfl_up_sync(FULL_MASK, pre, off);
+                    if (lane >= off) pre += y;
+                }
+                const unsigned hit = __ballot_sync(FULL_MASK, r < rend && dval + pre >= 0);
+                if (hit) {
+                    rstar = rb + __ffs(hit); // lane f (1-based) reaches row rb + f
+                    break;
+                }
+                dval += __shfl_sync(FULL_MASK, pre, 31);
+            }
+        }
+        dr = rstar - 1;
+        dc = rstar + E;
+        if (dr < 0 || dc > s) return;
+        delta = delta_at(A, T, o, dr, dc, lane);
+    }
+    if (lane != 0) return;
+    (void)G;
+    const int last = E + B;
+    while (dr >= 0 && dc <= s && dc - dr <= last) {
+        if (dc > 0) {
+            const int dl = delta - colinc(A, o, dc - 1, dr);
+            const int dd = delta + rowinc(A, o, dr, dc);
+            if (dl < 0 && dd > 0) A.res[o + dr] = dc - 1;
+        }
+        if (delta < 0) {
+            if (dc + 1 <= s) delta += colinc(A, o, dc, dr);
+            ++dc;
+        } else if (delta == 0) {
+            if (dr - 1 >= 0) delta -= rowinc(A, o, dr - 1, dc);
+            --dr;
+        } else {
+            break;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // staggered multiplication around the steady ant
 // ---------------------------------------------------------------------------
 // c2r = inverse of r2c; entries outside [0, n) raise *bad.  c2r must be -1 filled.
@@ -762,12 +1009,45 @@ __global__ void report_bad_kernel(const int32_t *bad, uint32_t *status)
 
 } // namespace
 
-slcs_status braid_workspace_bytes(int p, int q, int k, size_t *bytes)
+// Grid spacing and table stride of the concurrent walk at `level` (nodes of at
+// most smax entries).
+static void walk_grid(int k, int level, int &B, int &stride)
+{
+    int smax = k;
+    for (int d = 0; d < level; ++d) smax = smax - (smax >> 1);
+    B = std::max(WALK_BMIN, (smax + WALK_GMAX - 1) / WALK_GMAX);
+    stride = smax / B + 1;
+}
+
+// First level whose nodes are at most `cutoff` entries.
+static int cutoff_level(int k, int cutoff)
+{
+    int lc = 0;
+    for (int s = k; s > cutoff; s = s - (s >> 1)) ++lc;
+    return lc;
+}
+
+static size_t table_ints(int k, int cutoff)
+{
+    size_t best = 0;
+    const int lc = cutoff_level(k, cutoff);
+    for (int l = 0; l < lc; ++l) {
+        int B, stride;
+        walk_grid(k, l, B, stride);
+        best = std::max(best, (size_t(1) << l) * size_t(stride) * size_t(stride));
+    }
+    return best;
+}
+
+slcs_status braid_workspace_bytes(int p, int q, int k, int cutoff, size_t *bytes)
 {
     const int n = std::max(p, q);
     const int levels = braid_levels(k);
     const size_t kk = size_t(std::max(k, 1));
+    if (cutoff <= 0) cutoff = 1024;
+    if (cutoff > SUB_MAX) cutoff = SUB_MAX;
     size_t b = 0;
+    b += 2 * table_ints(k, cutoff) * sizeof(int32_t) + 512; // delta tables (hi, lo)
     b += 4 * kk * sizeof(int32_t);                         // P/Q ping-pong
     b += 2 * kk * size_t(levels + 2) * sizeof(int32_t);    // maps per level
     b += kk * size_t(levels + 2) * sizeof(int32_t);        // results per level
@@ -825,6 +1105,9 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     int32_t *map_row = reinterpret_cast<int32_t *>(take(kk * 4));
     int32_t *map_col = reinterpret_cast<int32_t *>(take(kk * 4));
     int32_t *bad = reinterpret_cast<int32_t *>(take(256));
+    const size_t tints = table_ints(k, cutoff);
+    int32_t *tab_hi = reinterpret_cast<int32_t *>(take(tints * 4));
+    int32_t *tab_lo = reinterpret_cast<int32_t *>(take(tints * 4));
     if (size_t(cur - static_cast<char *>(ws)) > ws_bytes) return fail(SLCS_ERR_ALLOC, "braid workspace too small");
 
     SLCS_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), st));
@@ -843,14 +1126,7 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         slice_write_kernel<<<nbs, 256, 0, st>>>(S);
     }
     // Levels above the cutoff: device-wide partitions.
-    int lc = 0; // first level whose nodes fit a block
-    {
-        int s = k;
-        while (s > cutoff) {
-            s = s - (s >> 1);
-            ++lc;
-        }
-    }
+    const int lc = cutoff_level(k, cutoff); // first level whose nodes fit a block
     const int kb = int((kk + SCAN_BS - 1) / SCAN_BS);
     for (int l = 0; l < lc; ++l) {
         LevelArgs A{Pcur, Qcur, Pnext, Qnext, maps + 2 * kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1) + kk,
@@ -882,7 +1158,23 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
                    C, Rr, H, HC, res + kk * size_t(l), k, l, bad};
         glue_kernel<<<blocks_for(k, 256), 256, 0, st>>>(G);
         union_kernel<<<blocks_for(k, 256), 256, 0, st>>>(C, res + kk * size_t(l), k, bad);
-        walk_seq_kernel<<<((1 << l) + 127) / 128, 128, 0, st>>>(G);
+        int B, stride;
+        walk_grid(k, l, B, stride);
+        const int nodes = 1 << l;
+        const size_t tbytes = size_t(nodes) * stride * stride * 4;
+        SLCS_CUDA(cudaMemsetAsync(tab_hi, 0, tbytes, st));
+        SLCS_CUDA(cudaMemsetAsync(tab_lo, 0, tbytes, st));
+        TableArgs TA{C, H, tab_hi, tab_lo, k, l, B, stride, bad};
+        table_count_kernel<<<blocks_for(k, 256), 256, 0, st>>>(TA);
+        const int rows = nodes * stride;
+        table_rows_kernel<<<(rows + 255) / 256, 256, 0, st>>>(TA, nodes);
+        table_cols_kernel<<<(rows + 255) / 256, 256, 0, st>>>(TA, nodes);
+        int smax = k;
+        for (int d = 0; d < l; ++d) smax = smax - (smax >> 1);
+        const int nseg = 2 * ((smax + B - 1) / B) + 2;
+        SegArgs SA{C, H, Rr, HC, tab_hi, res + kk * size_t(l), k, l, B, stride, nseg, bad};
+        const long warps = long(nodes) * nseg;
+        walk_segments_kernel<<<int((warps * 32 + 127) / 128), 128, 0, st>>>(SA, nodes);
     }
     AssembleArgs A{P, P_c2r, Q, res, map_row, map_col, out, p, q, k, row_glue, bad};
     assemble_kernel<<<blocks_for(long(p) + q + k, 256), 256, 0, st>>>(A);

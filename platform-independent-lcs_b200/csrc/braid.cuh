@@ -8,7 +8,7 @@ namespace slcs {
 // Recursion depth of a steady-ant product of size k (levels until size 1).
 int braid_levels(int k);
 // Device workspace of one product.
-slcs_status braid_workspace_bytes(int p, int q, int k, size_t *bytes);
+slcs_status braid_workspace_bytes(int p, int q, int k, int cutoff, size_t *bytes);
 // staggered_multiply<row_glue>(P, Q, k) of full permutations (row->col device
 // arrays); out receives p+q-k entries.  Nodes of at most `cutoff` entries are
 // finished by one block in shared memory.  `bad` is a device flag the launch

@@ -248,14 +248,14 @@ __global__ void __launch_bounds__(WARPS * 32) comb_wavefront_kernel(const CombLa
 // A segment of SEG lanes is a SEG-deep systolic pipeline like the wavefront
 // warp, but its column stream is the concatenation of many pairs: lane l is
 // always l blocks behind lane 0, and when a lane finishes the last block of
-// one pair it writes its h strands, loads the next pair's symbols (fetched one
-// pair ahead) and carries on.  The pipeline fills and drains once per segment
-// instead of once per pair.  Segment lane 0 takes pairs from a global ticket
-// counter one pair ahead and publishes them in a shared-memory ring; the
-// other lanes read the ring when they reach that pair.
+// one pair it writes its h strands and switches to the next pair.  The
+// pipeline fills and drains once per segment instead of once per pair.
+//
+// Each segment owns a list of pairs fixed when the plan was made (longest
+// processing time first over all resident segments), so every lane knows the
+// pair after its current one and loads that pair's descriptor and row symbols
+// one pair ahead: nothing on a switch waits for memory.
 // ---------------------------------------------------------------------------
-constexpr int SRING = 64; // ring slots per segment (> lanes a segment can lag)
-
 template <int TM>
 struct StreamTask {
     int pair; // -1: no more work
@@ -265,28 +265,48 @@ struct StreamTask {
     int32_t *v_out;
 };
 
+// The pair a lane combs next: descriptor words and its TM row symbols.
 template <int TM>
-__device__ __forceinline__ void load_task(const CombLaunch &L, int pair, StreamTask<TM> &T)
+struct NextPair {
+    int pair;
+    int4 d0, d1; // PairDev: a_off, b_off | out_off, m, n
+    uint32_t sym[TM / 4];
+};
+
+template <int TM>
+__device__ __forceinline__ void fetch_next(const CombLaunch &L, int pair, int r0, NextPair<TM> &N)
 {
-    T.pair = pair;
-    if (pair < 0) {
-        T.m = T.n = T.nb = 0;
-        return;
+    N.pair = pair;
+    if (pair < 0) return;
+    const int4 *pd = reinterpret_cast<const int4 *>(L.pairs + pair);
+    N.d0 = __ldg(pd);
+    N.d1 = __ldg(pd + 1);
+    const int64_t a_off = int64_t((uint64_t(uint32_t(N.d0.y)) << 32) | uint32_t(N.d0.x));
+    const int m = N.d1.z;
+    const uint8_t *a = L.a_blob + a_off + r0;
+    if (r0 + TM <= m && (reinterpret_cast<uintptr_t>(a) & 3) == 0) {
+#pragma unroll
+        for (int q = 0; q < TM / 4; ++q) N.sym[q] = __ldg(reinterpret_cast<const uint32_t *>(a) + q);
+    } else {
+#pragma unroll
+        for (int q = 0; q < TM / 4; ++q) {
+            uint32_t w = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (r0 + 4 * q + k < m) w |= uint32_t(__ldg(a + 4 * q + k)) << (8 * k);
+            N.sym[q] = w;
+        }
     }
-    const PairDev P = L.pairs[pair];
-    T.m = P.m;
-    T.n = P.n;
-    T.nb = (P.n + TN - 1) / TN;
-    T.b = L.b_blob + P.b_off;
-    T.h_out = L.out + P.out_off;
-    T.v_out = T.h_out + P.m;
 }
 
-// Rows [r0, r0+TM) of pair `pair`: symbols into av, start ids into hv.
+// Make the fetched pair current: rows r0.. get its symbols and start ids.
 template <int TM>
-__device__ __forceinline__ void load_rows(const CombLaunch &L, int pair, int m, int r0, int (&av)[TM], int (&hv)[TM])
+__device__ __forceinline__ void take_next(const CombLaunch &L, const NextPair<TM> &N, int r0, StreamTask<TM> &T,
+                                          int (&av)[TM], int (&hv)[TM])
 {
-    if (pair < 0 || r0 >= m) {
+    T.pair = N.pair;
+    if (N.pair < 0) {
+        T.m = T.n = T.nb = 0;
 #pragma unroll
         for (int k = 0; k < TM; ++k) {
             av[k] = -1;
@@ -294,44 +314,43 @@ __device__ __forceinline__ void load_rows(const CombLaunch &L, int pair, int m, 
         }
         return;
     }
-    const uint8_t *a = L.a_blob + L.pairs[pair].a_off + r0;
-    const bool full = r0 + TM <= m;
-    if (full && (TM % 4 == 0) && (reinterpret_cast<uintptr_t>(a) & 3) == 0) {
+    const int64_t b_off = int64_t((uint64_t(uint32_t(N.d0.w)) << 32) | uint32_t(N.d0.z));
+    const int64_t o_off = int64_t((uint64_t(uint32_t(N.d1.y)) << 32) | uint32_t(N.d1.x));
+    T.m = N.d1.z;
+    T.n = N.d1.w;
+    T.nb = (T.n + TN - 1) / TN;
+    T.b = L.b_blob + b_off;
+    T.h_out = L.out + o_off;
+    T.v_out = T.h_out + T.m;
 #pragma unroll
-        for (int q = 0; q < TM / 4; ++q) {
-            const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(a) + q);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) av[4 * q + k] = int((w >> (8 * k)) & 0xffu);
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < TM; ++k) av[k] = (r0 + k < m) ? int(__ldg(a + k)) : -1;
+    for (int k = 0; k < TM; ++k) {
+        const bool in = r0 + k < T.m;
+        av[k] = in ? int((N.sym[k / 4] >> (8 * (k % 4))) & 0xffu) : -1;
+        hv[k] = in ? (T.m - 1 - r0 - k) : INT_MIN;
     }
-#pragma unroll
-    for (int k = 0; k < TM; ++k) hv[k] = (r0 + k < m) ? (m - 1 - r0 - k) : INT_MIN;
 }
 
 template <int TM, int SEG>
-__device__ __forceinline__ void stream_segment(const BatchLaunch &B, int *ring, int lane)
+__device__ __forceinline__ void stream_segment(const BatchLaunch &B, int seg_id, int lane)
 {
     const CombLaunch &L = B.wf;
     const int sl = lane & (SEG - 1); // lane within the segment
-    int *ticket = L.counters + 2;
-
-    // Segment lane 0 publishes the first two pairs before anyone starts.
-    int next_ticket = 0;
-    if (sl == 0) {
-        const int t0 = atomicAdd(ticket, 1);
-        ring[0] = t0 < B.nstream ? B.stream_pairs[t0] : -1;
-        next_ticket = atomicAdd(ticket, 1);
+    const int r0 = sl * TM;
+    const int32_t *list = nullptr;
+    int count = 0;
+    if (seg_id < B.nseg) {
+        const int beg = B.seg_off[seg_id];
+        list = B.seg_list + beg;
+        count = B.seg_off[seg_id + 1] - beg;
     }
-    __syncwarp();
 
-    int q = 0; // index of this lane's current pair within the segment's stream
+    int q = 0; // index of this lane's current pair in the segment's list
     StreamTask<TM> T;
-    load_task<TM>(L, ring[0], T);
+    NextPair<TM> N;
     int av[TM], hv[TM];
-    load_rows<TM>(L, T.pair, T.m, sl * TM, av, hv);
+    fetch_next<TM>(L, count > 0 ? list[0] : -1, r0, N);
+    take_next<TM>(L, N, r0, T, av, hv);
+    fetch_next<TM>(L, count > 1 ? list[1] : -1, r0, N);
     int blk = -sl;
 
     int vc[TN];
@@ -384,23 +403,16 @@ __device__ __forceinline__ void stream_segment(const BatchLaunch &B, int *ring, 
         }
 
         if (busy && ++blk == T.nb) {
-            // This lane leaves pair q: write its h strands, move to pair q+1.
-            const int r0 = sl * TM;
+            // This lane leaves pair q: write its h strands, move to pair q+1
+            // (already fetched) and fetch pair q+2.
 #pragma unroll
             for (int k = 0; k < TM; ++k)
                 if (r0 + k < T.m) T.h_out[T.m - 1 - r0 - k] = hv[k];
             ++q;
-            if (sl == 0) {
-                ring[q & (SRING - 1)] = next_ticket < B.nstream ? B.stream_pairs[next_ticket] : -1;
-                next_ticket = next_ticket < B.nstream ? atomicAdd(ticket, 1) : next_ticket;
-            }
-            // Lane 0 wrote slot q in an earlier step (or just now for itself).
-            const int pair = ring[q & (SRING - 1)];
-            load_task<TM>(L, pair, T);
-            load_rows<TM>(L, T.pair, T.m, r0, av, hv);
+            take_next<TM>(L, N, r0, T, av, hv);
+            fetch_next<TM>(L, q + 1 < count ? list[q + 1] : -1, r0, N);
             blk = 0;
         }
-        __syncwarp();
     }
 }
 
@@ -408,11 +420,16 @@ template <int TM, int SEG, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) comb_batch_kernel(const BatchLaunch B)
 {
     __shared__ __align__(16) int4 wf_ring[WARPS][RING];
-    __shared__ int s_ring[WARPS][32 / SEG][SRING];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const CombLaunch &L = B.wf;
-    // Phase 1: stripes of multi-stripe pairs, whole warps, wavefront order.
+    // Phase 1: this warp's stream segments (lists fixed by the plan).
+    if (B.nseg > 0) {
+        const int seg_id = (blockIdx.x * WARPS + w) * (32 / SEG) + lane / SEG;
+        stream_segment<TM, SEG>(B, seg_id, lane);
+    }
+    // Phase 2: stripes of multi-stripe pairs, whole warps, wavefront order,
+    // taken dynamically so that they also absorb the stream phase's tail.
     for (;;) {
         int k = 0;
         if (lane == 0) k = ld_relaxed_gpu(L.counters + 1) ? INT_MAX : atomicAdd(L.counters, 1);
@@ -421,8 +438,6 @@ __global__ void __launch_bounds__(WARPS * 32) comb_batch_kernel(const BatchLaunc
         const int2 tk = L.tasks[k];
         comb_stripe<BATCH_WF_TM>(L, L.pairs[tk.x], L.scratch_off[tk.x], tk.y, k, wf_ring[w], lane);
     }
-    // Phase 2: single-stripe pairs streamed through segments.
-    if (B.nstream > 0) stream_segment<TM, SEG>(B, s_ring[w][lane / SEG], lane);
 }
 
 __global__ void strands_to_perm_kernel(const int32_t *__restrict__ h, int32_t m, const int32_t *__restrict__ v,
@@ -476,16 +491,14 @@ slcs_status launch_batch_variant(const BatchLaunch &B, cudaStream_t stream, int 
             if (occ < 1) occ = 1;
         }
     }
-    if (stream == PREPARE_ONLY) return SLCS_OK;
-    const long segs_per_block = long(WARPS) * (32 / SEG);
-    long want = (long(B.nstream) + segs_per_block - 1) / segs_per_block;
-    const long want_wf = (long(B.wf.ntasks) + WARPS - 1) / WARPS;
-    if (want_wf > want) want = want_wf;
-    long grid = long(sm_count()) * occ;
-    if (want < grid) grid = want;
+    if (stream == PREPARE_ONLY) {
+        if (grid_out) *grid_out = sm_count() * occ;
+        return SLCS_OK;
+    }
+    int grid = B.grid;
     if (grid < 1) grid = 1;
-    comb_batch_kernel<TM, SEG, WARPS><<<int(grid), WARPS * 32, 0, stream>>>(B);
-    if (grid_out) *grid_out = int(grid);
+    comb_batch_kernel<TM, SEG, WARPS><<<grid, WARPS * 32, 0, stream>>>(B);
+    if (grid_out) *grid_out = grid;
     SLCS_CUDA(cudaGetLastError());
     return SLCS_OK;
 }
@@ -499,12 +512,12 @@ bool stream_variant_supported(int tm, int seg)
 
 slcs_status launch_batch(const BatchLaunch &B, int tm, int seg, cudaStream_t stream, int *grid_out)
 {
-    if (B.wf.ntasks <= 0 && B.nstream <= 0) return SLCS_OK;
+    if (stream != PREPARE_ONLY && B.wf.ntasks <= 0 && B.nseg <= 0) return SLCS_OK;
 #define SLCS_SEG_CASE(TM)                                                               \
     case TM:                                                                            \
-        if (seg == 8) return launch_batch_variant<TM, 8, 4>(B, stream, grid_out);       \
-        if (seg == 16) return launch_batch_variant<TM, 16, 4>(B, stream, grid_out);     \
-        return launch_batch_variant<TM, 32, 4>(B, stream, grid_out);
+        if (seg == 8) return launch_batch_variant<TM, 8, BATCH_WARPS>(B, stream, grid_out);   \
+        if (seg == 16) return launch_batch_variant<TM, 16, BATCH_WARPS>(B, stream, grid_out); \
+        return launch_batch_variant<TM, 32, BATCH_WARPS>(B, stream, grid_out);
     if (!stream_variant_supported(tm, seg)) return fail(SLCS_ERR_UNSUPPORTED, "stream tile_m/seg not supported");
     switch (tm) {
         SLCS_SEG_CASE(4)

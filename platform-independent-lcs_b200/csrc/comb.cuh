@@ -30,9 +30,11 @@ struct CombLaunch {
 // streamed: a segment of `seg` lanes combs pair after pair without draining
 // its pipeline between them.
 struct BatchLaunch {
-    CombLaunch wf;              // wavefront part (tasks of multi-stripe pairs)
-    const int32_t *stream_pairs; // device: single-stripe pairs, largest first
-    int32_t nstream;
+    CombLaunch wf;           // wavefront part (tasks of multi-stripe pairs)
+    const int32_t *seg_off;  // device: nseg+1 offsets into seg_list (CSR)
+    const int32_t *seg_list; // device: pairs of each stream segment, in order
+    int32_t nseg;            // stream segments with a list (may be 0)
+    int32_t grid;            // blocks of the persistent launch
 };
 
 // Rows of a one lane keeps in registers; supported values.
@@ -55,9 +57,11 @@ slcs_status launch_comb(const CombLaunch &L, int tile_m, int warps, cudaStream_t
 
 // Stream-mode variants: rows per lane and lanes per segment.
 bool stream_variant_supported(int stream_tm, int seg);
-// Enqueue one persistent batch launch (counters [0] wavefront ticket, [1]
-// abort, [2] stream ticket must be zero).  Wavefront tasks use tile_m 8.
+// Enqueue one persistent batch launch (counters [0] wavefront ticket and [1]
+// abort must be zero).  Wavefront tasks use tile_m 8.  With PREPARE_ONLY as
+// the stream, *grid_out receives the full persistent grid (blocks).
 slcs_status launch_batch(const BatchLaunch &L, int stream_tm, int seg, cudaStream_t stream, int *grid_out);
+constexpr int BATCH_WARPS = 4;
 constexpr int BATCH_WF_TM = 8;
 
 // Strands -> permutation matrix arrays (either output may be null).

@@ -2,6 +2,7 @@
 
     python -m slcs.profile_case batch [npairs]     # one batch launch (read/window pairs)
     python -m slcs.profile_case pair  [length]     # one square uniform pair
+    python -m slcs.profile_case braid [k] [cutoff] # one staggered product of overlap k
 
 Each case runs one warm-up launch and then the launch to capture, and checks
 the device status word; it holds a few hundred MB on the device at most.
@@ -23,7 +24,7 @@ def main():
     if kind == "batch":
         batch = W.reads_20000(npairs=size or 20000)
         _, total = batch.strand_offsets()
-        cfg = slcs.Config.make(tile_m=tm or 8)
+        cfg = slcs.Config.make(tile_m=tm or None)
         plan = slcs.BatchPlan(slcs.pair_descs(batch), cfg)
         a = torch.from_numpy(batch.a_blob).to(dev)
         b = torch.from_numpy(batch.b_blob).to(dev)
@@ -38,9 +39,18 @@ def main():
         a = torch.from_numpy(rng.integers(0, 4, n, dtype=np.uint8)).to(dev)
         b = torch.from_numpy(rng.integers(0, 4, n, dtype=np.uint8)).to(dev)
         out = torch.empty(2 * n, dtype=torch.int32, device=dev)
-        cfg = slcs.Config.make(tile_m=tm or 16)
+        cfg = slcs.Config.make(tile_m=tm or 16, wait_ms=600000)
         for _ in range(2):
             slcs.comb_pair(a, b, cfg=cfg, out=out)
+        torch.cuda.synchronize()
+    elif kind == "braid":
+        k = size or (1 << 18)
+        rng = np.random.default_rng(2)
+        P = torch.from_numpy(rng.permutation(k + 1000).astype(np.int32)).to(dev)
+        Q = torch.from_numpy(rng.permutation(k + 3000).astype(np.int32)).to(dev)
+        cfg = slcs.Config.make(braid_cutoff=tm or None)
+        for _ in range(2):
+            slcs.braid_multiply(P, Q, k, False, cfg=cfg)
         torch.cuda.synchronize()
     else:
         raise SystemExit(f"unknown case {kind}")
