@@ -104,6 +104,25 @@ SLCS_API slcs_status slcs_device_name(int32_t device, char *buf, int32_t len);
 SLCS_API slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n,
                            int32_t *h_out, int32_t *v_out, const slcs_config *cfg, void *stream);
 
+/* One pair, device pointers, without allocating anything.  No counterpart in
+ * the reference; it exists for callers that cannot allocate device memory at
+ * call time (a stream being captured into a CUDA graph with allocation
+ * disallowed, a service that reserves all memory up front).  The scratch that
+ * slcs_comb_pair allocates lives here in one fixed device array of
+ * SLCS_NOALLOC_SCRATCH_BYTES (held by every GPU that loads the library until
+ * exit); a pair needing more scratch than that (about 4 bytes per column of b
+ * when a has more than 32*tile_m rows, plus 4 bytes per row stripe) is refused
+ * with SLCS_ERR_RANGE.  strands_out holds h (m entries) followed by v (n).
+ * The first call on a device looks up the array's address (do it before any
+ * stream capture).  Every call shares the one array, so calls whose work can
+ * overlap on the GPU (different streams, or before the previous call's kernel
+ * finished on another stream) race; serialise them.  Device-side wait
+ * timeouts raise slcs_device_status() only if an earlier call on this device
+ * created the status word. */
+#define SLCS_NOALLOC_SCRATCH_BYTES (16u << 20)
+SLCS_API slcs_status slcs_comb_pair_noalloc(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n,
+                                            int32_t *strands_out, const slcs_config *cfg, void *stream);
+
 /* One pair, host pointers (copies in, combs, copies out, synchronises).  The
  * entry point a SemiLocalLcsImpl adapter (src/algorithm_registry.cpp:59-73)
  * binds. */

@@ -140,6 +140,13 @@ slcs_status cuda_fail(cudaError_t e, const char *what)
     return SLCS_ERR_DEVICE;
 }
 uint32_t *device_status_word() { return dev_state().dev_status; }
+uint32_t *device_status_word_if_ready()
+{
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) return nullptr;
+    std::lock_guard<std::mutex> g(g_dev_mu);
+    return g_dev[d].init ? g_dev[d].dev_status : nullptr;
+}
 int sm_count() { return dev_state().sms; }
 
 // Pairs with an empty side have no cells: the strands keep their start ids.

@@ -503,7 +503,52 @@ slcs_status launch_batch_variant(const BatchLaunch &B, cudaStream_t stream, int 
     return SLCS_OK;
 }
 
+// The wavefront launch with the SM count given by the caller (used by the
+// entry point that must not allocate, so it cannot touch the lazily created
+// per-device state behind sm_count()).
+template <int TM, int WARPS>
+slcs_status launch_variant_on(const CombLaunch &L, int sms, cudaStream_t stream)
+{
+    static int occ = -1;
+    static std::mutex mu;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (occ < 0) {
+            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WARPS>,
+                                                                    WARPS * 32, 0));
+            if (occ < 1) occ = 1;
+        }
+    }
+    const long want = (long(L.ntasks) + WARPS - 1) / WARPS;
+    long grid = long(sms > 0 ? sms : 1) * occ;
+    if (want < grid) grid = want;
+    if (grid < 1) grid = 1;
+    comb_wavefront_kernel<TM, WARPS><<<int(grid), WARPS * 32, 0, stream>>>(L);
+    SLCS_CUDA(cudaGetLastError());
+    return SLCS_OK;
+}
+
 } // namespace
+
+slcs_status launch_comb_on(const CombLaunch &L, int tile_m, int warps, int sms, cudaStream_t stream)
+{
+    if (L.ntasks <= 0) return SLCS_OK;
+#define SLCS_TM_ON(TM)                                                                     \
+    case TM:                                                                               \
+        if (warps == 2) return launch_variant_on<TM, 2>(L, sms, stream);                   \
+        if (warps == 8) return launch_variant_on<TM, 8>(L, sms, stream);                   \
+        return launch_variant_on<TM, 4>(L, sms, stream);
+    switch (tile_m) {
+        SLCS_TM_ON(2)
+        SLCS_TM_ON(4)
+        SLCS_TM_ON(8)
+        SLCS_TM_ON(12)
+        SLCS_TM_ON(16)
+    default:
+        return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+    }
+#undef SLCS_TM_ON
+}
 
 bool stream_variant_supported(int tm, int seg)
 {

@@ -55,6 +55,9 @@ static const cudaStream_t PREPARE_ONLY = reinterpret_cast<cudaStream_t>(~uintptr
 // Enqueue one persistent launch; `counters` and `progress` must be zero.
 slcs_status launch_comb(const CombLaunch &L, int tile_m, int warps, cudaStream_t stream, int *grid_out);
 
+// launch_comb with the SM count supplied by the caller (no per-device state).
+slcs_status launch_comb_on(const CombLaunch &L, int tile_m, int warps, int sms, cudaStream_t stream);
+
 // Stream-mode variants: rows per lane and lanes per segment.
 bool stream_variant_supported(int stream_tm, int seg);
 // Enqueue one persistent batch launch (counters [0] wavefront ticket and [1]

@@ -49,6 +49,8 @@ slcs_status cuda_fail(cudaError_t e, const char *what);
 
 // Mapped pinned status word of the current device (device-visible pointer).
 uint32_t *device_status_word();
+// The same word if an earlier call already created it, else null (never allocates).
+uint32_t *device_status_word_if_ready();
 int sm_count();
 
 // ---- device helpers ---------------------------------------------------------
