@@ -65,7 +65,8 @@ typedef struct {
     int32_t use_graph;     /* batch plans: replay the launch as a captured CUDA graph */
     int32_t seg;           /* batch stream mode: lanes per pipeline segment (8/16/32) */
     int32_t wait_ms;       /* limit of one device-side wait (default 10000 ms)        */
-    int32_t reserved[7];
+    int32_t blocks_per_sm; /* batch plans: resident blocks per SM (default: occupancy) */
+    int32_t reserved[6];
 } slcs_config;
 
 /* One pair of a batch: symbols at a_blob[a_offset .. +m) and b_blob[b_offset .. +n);
@@ -159,13 +160,16 @@ SLCS_API int32_t slcs_batch_plan_launches(const slcs_batch_plan *plan);
 
 /* What a plan decided: the kernel variant and how the pairs were split. */
 typedef struct {
-    int32_t stream_tile_m;   /* rows per lane of streamed pairs (0: wavefront only) */
-    int32_t seg;             /* lanes per stream segment                            */
+    int32_t stream_tile_m;   /* rows per lane of the tallest stream class (0: wavefront only) */
+    int32_t seg;             /* lanes per segment of that class                     */
     int32_t wavefront_tile_m;/* rows per lane of wavefront stripes                  */
     int32_t warps;           /* warps per block                                     */
     int32_t stream_pairs;    /* pairs combed in stream mode                         */
     int32_t wavefront_tasks; /* row stripes combed as wavefront tasks               */
-    int32_t reserved[2];
+    int32_t stream_classes;  /* stream classes in use                               */
+    int32_t tile_n;          /* stream columns per step                             */
+    int32_t grid;            /* blocks of the launch                                */
+    int32_t reserved[3];
 } slcs_plan_info;
 SLCS_API slcs_status slcs_batch_plan_info(const slcs_batch_plan *plan, slcs_plan_info *info);
 
@@ -189,6 +193,32 @@ SLCS_API int64_t slcs_permutation_hash(const int32_t *col_to_row, int32_t size);
 SLCS_API slcs_status slcs_braid_multiply(const int32_t *p_row_to_col, int32_t p_size, const int32_t *q_row_to_col,
                                 int32_t q_size, int32_t k, int32_t row_glue, int32_t *out_row_to_col,
                                 const slcs_config *cfg, void *stream);
+
+/* ---- cost model (no counterpart in the reference) ---------------------- */
+
+/* A 4 -> 64 -> 64 -> k FP32 MLP predicting the log2 run time of k kernel
+ * variants from (log2 m, log2 n, log2 alphabet, log2 batch).  Trained and
+ * evaluated on the current device by hand-written kernels; all arrays are
+ * host arrays.  The model only chooses launch parameters, never results. */
+#define SLCS_MLP_FEATURES 4
+#define SLCS_MLP_HIDDEN 64
+#define SLCS_MLP_MAX_OUTPUTS 32
+/* Floats in the parameter blob for k outputs (0 when k is out of range). */
+SLCS_API int32_t slcs_costmodel_param_count(int32_t k);
+/* He-initialised parameters; feat_mean/feat_std normalise the 4 features. */
+SLCS_API slcs_status slcs_costmodel_init(float *params, int32_t k, uint64_t seed, const float *feat_mean,
+                                         const float *feat_std);
+/* `epochs` full-batch Adam steps on (X [n x 4], T [n x k]) where mask != 0;
+ * params are updated in place; *loss_out = mean squared error of the last
+ * step. */
+SLCS_API slcs_status slcs_costmodel_train(float *params, int32_t k, const float *X, const float *T,
+                                          const uint8_t *mask, int32_t n, int32_t epochs, float lr,
+                                          float *loss_out);
+/* Y [n x k] = model(X). */
+SLCS_API slcs_status slcs_costmodel_predict(const float *params, int32_t k, const float *X, int32_t n, float *Y);
+/* One forward + backward pass: d(loss)/d(params) (mean/std slots are 0). */
+SLCS_API slcs_status slcs_costmodel_grad(const float *params, int32_t k, const float *X, const float *T,
+                                         const uint8_t *mask, int32_t n, float *grad_out, float *loss_out);
 
 /* ---- diagnostics (no counterpart in the reference) --------------------- */
 

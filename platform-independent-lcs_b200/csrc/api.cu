@@ -171,7 +171,13 @@ struct slcs_batch_plan {
     int32_t npairs = 0;
     int32_t ntasks = 0;
     int32_t nstream = 0;
-    int32_t nseg = 0;   // stream segments with a pair list
+    int tns = 8;        // stream columns per step
+    int blocks_per_sm = 0;
+    std::vector<std::pair<int, int>> classes; // stream classes (rows per lane, lanes per segment)
+    int32_t nclass = 0; // classes with warps
+    int32_t class_warp_end[MAX_CLASSES] = {};
+    int32_t class_code[MAX_CLASSES] = {};
+    int32_t nwarps = 0; // warps with a stream class
     int grid = 0;       // blocks of the batch launch
     uint64_t wait_ns = DEFAULT_WAIT_NS;
     bool use_graph = false;
@@ -216,8 +222,12 @@ struct slcs_batch_plan {
         SLCS_CUDA(cudaMemsetAsync(d_work, 0, work_bytes, st));
         slcs_status s;
         if (stm > 0) {
-            BatchLaunch B{launch(a, b, out), d_seg_off, d_seg_list, nseg, grid};
-            s = launch_batch(B, stm, seg, st, nullptr);
+            BatchLaunch B{launch(a, b, out), d_seg_off, d_seg_list, nwarps, grid, nclass, {}, {}};
+            for (int c = 0; c < nclass; ++c) {
+                B.class_warp_end[c] = class_warp_end[c];
+                B.class_code[c] = class_code[c];
+            }
+            s = launch_batch(B, tns, st, nullptr);
         } else {
             s = launch_comb(launch(a, b, out), tm, warps, st, nullptr);
         }
@@ -416,31 +426,31 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
             return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
         }
     } else {
-        // Stream mode: single-stripe pairs stream through segments; larger
-        // pairs run as wavefront tasks of BATCH_WF_TM rows per lane.
+        // Stream mode: pairs of at most 512 rows stream through segments,
+        // each pair in the smallest class whose segment holds all its rows;
+        // taller pairs run as wavefront tasks of BATCH_WF_TM rows per lane.
+        // A configuration naming tile_m (and seg) asks for that one class.
         P->tm = BATCH_WF_TM;
-        P->seg = (cfg && cfg->seg) ? cfg->seg : 16;
+        P->tns = (cfg && cfg->tile_n) ? cfg->tile_n : 8;
+        if (P->tns != 4 && P->tns != 8) {
+            delete P;
+            return fail(SLCS_ERR_UNSUPPORTED, "stream mode needs tile_n 4 or 8");
+        }
         if (cfg && cfg->tile_m) {
             P->stm = cfg->tile_m;
+            P->seg = cfg->seg ? cfg->seg : 16;
+            P->classes = {{P->stm, P->seg}};
         } else {
-            // Fixed heuristic: the smallest rows-per-lane whose segment holds
-            // nine pairs in ten whole.
-            int32_t p90 = 0;
-            if (!ms.empty()) {
-                std::nth_element(ms.begin(), ms.begin() + (ms.size() * 9) / 10, ms.end());
-                p90 = ms[(ms.size() * 9) / 10];
-            }
             P->stm = 16;
-            for (int t : {4, 8, 12, 16})
-                if (P->seg * t >= p90) {
-                    P->stm = t;
-                    break;
-                }
+            P->seg = 16;
+            P->classes = {{4, 16}, {8, 16}, {12, 16}, {16, 16}, {16, 32}};
         }
-        if (!stream_variant_supported(P->stm, P->seg)) {
-            delete P;
-            return fail(SLCS_ERR_UNSUPPORTED, "stream mode needs tile_m in {4,8,12,16} and seg in {8,16,32}");
-        }
+        for (const auto &c : P->classes)
+            if (!stream_variant_supported(c.first, c.second)) {
+                delete P;
+                return fail(SLCS_ERR_UNSUPPORTED, "stream mode needs tile_m in {4,8,12,16} and seg in {8,16,32}");
+            }
+        P->blocks_per_sm = (cfg && cfg->blocks_per_sm > 0) ? cfg->blocks_per_sm : 0;
     }
     for (int32_t p = 0; p < npairs; ++p) {
         if (pairs[p].m == 0 || pairs[p].n == 0) P->empty_pairs.push_back(pairs[p]);
@@ -448,7 +458,9 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
         P->need_b = std::max<int64_t>(P->need_b, pairs[p].b_offset + pairs[p].n);
         P->need_out = std::max<int64_t>(P->need_out, pairs[p].out_offset + pairs[p].m + pairs[p].n);
     }
-    Schedule S = build_schedule(pairs, npairs, P->tm, P->stm > 0 ? P->seg * P->stm : 0);
+    int32_t stream_rows = 0;
+    for (const auto &c : P->classes) stream_rows = std::max(stream_rows, c.first * c.second);
+    Schedule S = build_schedule(pairs, npairs, P->tm, stream_rows);
     P->ntasks = int32_t(S.tasks.size());
     // One-time device set-up now, so a graph capture in run() issues only
     // capturable work: the mapped status word and the occupancy queries.
@@ -457,8 +469,7 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
     {
         CombLaunch dummy{};
         dummy.ntasks = 1;
-        slcs_status ps = P->stm > 0 ? launch_batch(BatchLaunch{dummy, nullptr, nullptr, 0, 0}, P->stm, P->seg,
-                                                   PREPARE_ONLY, &full_grid)
+        slcs_status ps = P->stm > 0 ? launch_batch(BatchLaunch{dummy}, P->tns, PREPARE_ONLY, &full_grid)
                                     : launch_comb(dummy, P->tm, P->warps, PREPARE_ONLY, nullptr);
         if (ps != SLCS_OK) {
             delete P;
@@ -466,35 +477,86 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
         }
     }
     P->nstream = int32_t(S.stream_pairs.size());
-    // Stream segments and their pair lists: longest processing time first
-    // (a pair costs its column blocks plus the switch), each pair to the least
-    // loaded segment; the grid is the persistent one, or fewer blocks when the
-    // batch is small.
+    // Stream classes, warps and pair lists.  A pair costs its column blocks
+    // plus a switch; each class gets warps in proportion to its cost per
+    // warp (a warp runs 32/seg segments side by side), and within a class
+    // the pairs go longest first to the least loaded segment.  The grid is
+    // the persistent one (or blocks_per_sm per SM), fewer for small batches.
     std::vector<int32_t> seg_off, seg_list;
     if (P->stm > 0) {
-        const int segs_per_block = BATCH_WARPS * (32 / P->seg);
-        int grid = std::max(1, full_grid);
-        const long want_stream = (long(P->nstream) + segs_per_block - 1) / segs_per_block;
+        const int occ_blocks = std::max(1, full_grid / std::max(1, sm_count()));
+        int grid = sm_count() * (P->blocks_per_sm > 0 ? std::min(P->blocks_per_sm, occ_blocks) : occ_blocks);
+        const int nclass = int(P->classes.size());
+        std::vector<std::vector<int32_t>> cls_pairs(nclass);
+        for (int32_t p : S.stream_pairs) { // largest first
+            int c = 0;
+            while (c < nclass - 1 && pairs[p].m > P->classes[c].first * P->classes[c].second) ++c;
+            cls_pairs[c].push_back(p);
+        }
+        auto cost = [&](int32_t p) { return int64_t((pairs[p].n + P->tns - 1) / P->tns) + 2; };
+        std::vector<double> wsteps(nclass, 0.0);
+        std::vector<long> wmax(nclass, 0);
+        double total = 0.0;
+        for (int c = 0; c < nclass; ++c) {
+            int64_t w = 0;
+            for (int32_t p : cls_pairs[c]) w += cost(p);
+            const int spw = 32 / P->classes[c].second;
+            wsteps[c] = double(w) / spw;
+            wmax[c] = (long(cls_pairs[c].size()) + spw - 1) / spw;
+            total += wsteps[c];
+        }
         const long want_wf = (long(P->ntasks) + BATCH_WARPS - 1) / BATCH_WARPS;
-        grid = int(std::min<long>(grid, std::max<long>(1, std::max(want_stream, want_wf))));
-        P->grid = grid;
-        P->nseg = P->nstream > 0 ? int32_t(std::min<long>(long(grid) * segs_per_block, P->nstream)) : 0;
-        if (P->nseg > 0) {
-            std::vector<std::vector<int32_t>> lists(P->nseg);
-            using Load = std::pair<int64_t, int32_t>;
+        long want = std::max<long>(1, want_wf);
+        long sum_wmax = 0;
+        for (int c = 0; c < nclass; ++c) sum_wmax += wmax[c];
+        want = std::max(want, (sum_wmax + BATCH_WARPS - 1) / BATCH_WARPS);
+        grid = int(std::max<long>(1, std::min<long>(grid, want)));
+        const long warps_total = long(grid) * BATCH_WARPS;
+        std::vector<long> wc(nclass, 0);
+        long used = 0;
+        for (int c = 0; c < nclass; ++c) {
+            if (cls_pairs[c].empty()) continue;
+            long w = total > 0 ? long(double(warps_total) * wsteps[c] / total) : 1;
+            w = std::max(1L, std::min(w, wmax[c]));
+            wc[c] = w;
+            used += w;
+        }
+        while (used > warps_total) { // trim the largest allocations
+            int big = int(std::max_element(wc.begin(), wc.end()) - wc.begin());
+            if (wc[big] <= 1) break;
+            --wc[big];
+            --used;
+        }
+        P->grid = int(std::max<long>(grid, (used + BATCH_WARPS - 1) / BATCH_WARPS));
+        P->nclass = 0;
+        long wbase = 0;
+        std::vector<std::vector<int32_t>> slot_lists(size_t(std::max(used, 1L)) * SEG_SLOTS);
+        for (int c = 0; c < nclass; ++c) {
+            if (wc[c] == 0) continue;
+            const int spw = 32 / P->classes[c].second;
+            const long nseg = wc[c] * spw;
+            using Load = std::pair<int64_t, int64_t>;
             std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
-            for (int32_t sgi = 0; sgi < P->nseg; ++sgi) heap.push({0, sgi});
-            for (int32_t p : S.stream_pairs) { // already largest first
+            for (long sgi = 0; sgi < nseg; ++sgi) heap.push({0, sgi});
+            for (int32_t p : cls_pairs[c]) {
                 Load top = heap.top();
                 heap.pop();
-                lists[top.second].push_back(p);
-                top.first += (pairs[p].n + 3) / 4 + 2;
+                const long warp = wbase + top.second / spw, s = top.second % spw;
+                slot_lists[size_t(warp) * SEG_SLOTS + size_t(s)].push_back(p);
+                top.first += cost(p);
                 heap.push(top);
             }
-            seg_off.reserve(P->nseg + 1);
+            wbase += wc[c];
+            P->class_warp_end[P->nclass] = int32_t(wbase);
+            P->class_code[P->nclass] = P->classes[c].first * 100 + P->classes[c].second;
+            ++P->nclass;
+        }
+        P->nwarps = int32_t(wbase);
+        if (P->nwarps > 0) {
+            seg_off.reserve(size_t(P->nwarps) * SEG_SLOTS + 1);
             seg_off.push_back(0);
-            for (auto &l : lists) {
-                seg_list.insert(seg_list.end(), l.begin(), l.end());
+            for (long sl = 0; sl < long(P->nwarps) * SEG_SLOTS; ++sl) {
+                seg_list.insert(seg_list.end(), slot_lists[size_t(sl)].begin(), slot_lists[size_t(sl)].end());
                 seg_off.push_back(int32_t(seg_list.size()));
             }
         }
@@ -535,6 +597,9 @@ slcs_status slcs_batch_plan_info(const slcs_batch_plan *P, slcs_plan_info *info)
     std::memset(info, 0, sizeof(*info));
     info->stream_tile_m = P->stm;
     info->seg = P->stm > 0 ? P->seg : 0;
+    info->stream_classes = P->nclass;
+    info->tile_n = P->stm > 0 ? P->tns : 4;
+    info->grid = P->grid;
     info->wavefront_tile_m = P->tm;
     info->warps = P->warps;
     info->stream_pairs = P->nstream;

@@ -642,53 +642,85 @@ __global__ void __launch_bounds__(256) table_count_kernel(TableArgs A)
     }
 }
 
-// Per (node, row block): exclusive prefix of hi counts and inclusive suffix of
-// lo counts along the columns.
+// One warp per (node, row block): exclusive prefix of the hi counts and
+// inclusive suffix of the lo counts along the row, 32 columns per step.
 __global__ void __launch_bounds__(256) table_rows_kernel(TableArgs A, int nodes)
 {
     if (*A.bad) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nodes * A.stride) return;
-    const int nd = t / A.stride, bi = t % A.stride;
+    const int lane = threadIdx.x & 31;
+    const long wid = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (wid >= long(nodes) * A.stride) return;
+    const int nd = int(wid / A.stride), bi = int(wid % A.stride);
     int o, s;
     node_by_index(nd, A.level, A.k, o, s);
     const int G = s / A.B;
     if (bi > G) return;
     int32_t *hi = A.cnt_hi + size_t(nd) * A.stride * A.stride + size_t(bi) * A.stride;
     int32_t *lo = A.cnt_lo + size_t(nd) * A.stride * A.stride + size_t(bi) * A.stride;
-    int run = 0;
-    for (int j = 0; j <= G; ++j) {
-        const int v = hi[j];
-        hi[j] = run;
-        run += v;
+    int carry = 0;
+    for (int base = 0; base <= G; base += 32) {
+        const int j = base + lane;
+        const int v = j <= G ? hi[j] : 0;
+        int x = v;
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(FULL_MASK, x, off);
+            if (lane >= off) x += y;
+        }
+        if (j <= G) hi[j] = carry + x - v;
+        carry += __shfl_sync(FULL_MASK, x, 31);
     }
-    run = 0;
-    for (int j = G; j >= 0; --j) {
-        run += lo[j];
-        lo[j] = run;
+    carry = 0;
+    for (int base = (G / 32) * 32; base >= 0; base -= 32) {
+        const int j = base + lane;
+        int x = j <= G ? lo[j] : 0; // becomes the sum over lanes >= lane
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_down_sync(FULL_MASK, x, off);
+            if (lane + off < 32) x += y;
+        }
+        if (j <= G) lo[j] = carry + x;
+        carry += __shfl_sync(FULL_MASK, x, 0);
     }
 }
 
-// Per (node, grid column): finish the 2D sums and store the delta table.
-__global__ void __launch_bounds__(256) table_cols_kernel(TableArgs A, int nodes)
+// One block per (node, 32 grid columns): a three-phase scan down the rows
+// (32 row chunks per column, coalesced across the columns) that finishes the
+// 2D sums and stores delta(iB, jB) = hi-prefix - lo-suffix in the hi table.
+__global__ void __launch_bounds__(1024) table_cols_kernel(TableArgs A, int nodes)
 {
     if (*A.bad) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nodes * A.stride) return;
-    const int nd = t / A.stride, j = t % A.stride;
+    const int colblocks = (A.stride + 31) / 32;
+    const int nd = blockIdx.x / colblocks, jb = blockIdx.x % colblocks;
     int o, s;
     node_by_index(nd, A.level, A.k, o, s);
     const int G = s / A.B;
-    if (j > G) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int j = jb * 32 + tx;
+    const bool col_ok = j <= G;
+    const int rows = G + 1, per = (rows + 31) / 32;
+    const int i0 = min(rows, ty * per), i1 = min(rows, i0 + per);
     int32_t *hi = A.cnt_hi + size_t(nd) * A.stride * A.stride + j;
     int32_t *lo = A.cnt_lo + size_t(nd) * A.stride * A.stride + j;
-    int run = 0;
-    for (int i = G; i >= 0; --i) {
+    __shared__ int Hs[32][33], Ls[32][33];
+    int hs = 0, ls = 0;
+    if (col_ok)
+        for (int i = i0; i < i1; ++i) {
+            hs += hi[size_t(i) * A.stride];
+            ls += lo[size_t(i) * A.stride];
+        }
+    Hs[ty][tx] = hs;
+    Ls[ty][tx] = ls;
+    __syncthreads();
+    int hoff = 0, loff = 0;
+    for (int t = 0; t < ty; ++t) hoff += Hs[t][tx];
+    for (int t = ty + 1; t < 32; ++t) loff += Ls[t][tx];
+    if (!col_ok) return;
+    int run = loff;
+    for (int i = i1 - 1; i >= i0; --i) {
         run += lo[size_t(i) * A.stride];
-        lo[size_t(i) * A.stride] = run; // lo[i][j] = #lo points with row >= iB, col >= jB
+        lo[size_t(i) * A.stride] = run; // #lo points with row >= iB, col >= jB
     }
-    run = 0;
-    for (int i = 0; i <= G; ++i) {
+    run = hoff;
+    for (int i = i0; i < i1; ++i) {
         const int v = hi[size_t(i) * A.stride];
         hi[size_t(i) * A.stride] = run - lo[size_t(i) * A.stride]; // delta(iB, jB)
         run += v;
@@ -1167,8 +1199,8 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         TableArgs TA{C, H, tab_hi, tab_lo, k, l, B, stride, bad};
         table_count_kernel<<<blocks_for(k, 256), 256, 0, st>>>(TA);
         const int rows = nodes * stride;
-        table_rows_kernel<<<(rows + 255) / 256, 256, 0, st>>>(TA, nodes);
-        table_cols_kernel<<<(rows + 255) / 256, 256, 0, st>>>(TA, nodes);
+        table_rows_kernel<<<int((long(rows) * 32 + 255) / 256), 256, 0, st>>>(TA, nodes);
+        table_cols_kernel<<<nodes * ((stride + 31) / 32), 1024, 0, st>>>(TA, nodes);
         int smax = k;
         for (int d = 0; d < l; ++d) smax = smax - (smax >> 1);
         const int nseg = 2 * ((smax + B - 1) / B) + 2;

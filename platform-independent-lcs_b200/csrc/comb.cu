@@ -330,19 +330,15 @@ __device__ __forceinline__ void take_next(const CombLaunch &L, const NextPair<TM
     }
 }
 
-template <int TM, int SEG>
+template <int TM, int SEG, int TNS>
 __device__ __forceinline__ void stream_segment(const BatchLaunch &B, int seg_id, int lane)
 {
     const CombLaunch &L = B.wf;
     const int sl = lane & (SEG - 1); // lane within the segment
     const int r0 = sl * TM;
-    const int32_t *list = nullptr;
-    int count = 0;
-    if (seg_id < B.nseg) {
-        const int beg = B.seg_off[seg_id];
-        list = B.seg_list + beg;
-        count = B.seg_off[seg_id + 1] - beg;
-    }
+    const int beg = B.seg_off[seg_id];
+    const int32_t *list = B.seg_list + beg;
+    const int count = B.seg_off[seg_id + 1] - beg;
 
     int q = 0; // index of this lane's current pair in the segment's list
     StreamTask<TM> T;
@@ -350,45 +346,49 @@ __device__ __forceinline__ void stream_segment(const BatchLaunch &B, int seg_id,
     int av[TM], hv[TM];
     fetch_next<TM>(L, count > 0 ? list[0] : -1, r0, N);
     take_next<TM>(L, N, r0, T, av, hv);
+    T.nb = (T.n + TNS - 1) / TNS;
     fetch_next<TM>(L, count > 1 ? list[1] : -1, r0, N);
     int blk = -sl;
 
-    int vc[TN];
+    int vc[TNS];
 #pragma unroll
-    for (int j = 0; j < TN; ++j) vc[j] = INT_MAX;
+    for (int j = 0; j < TNS; ++j) vc[j] = INT_MAX;
 
-    for (;;) {
-        const bool busy = T.pair >= 0;
-        if (!__any_sync(FULL_MASK, busy)) break;
-        const bool act = busy && blk >= 0;
+    for (int it = 0;; ++it) {
+        const bool live = T.pair >= 0;
+        if ((it & 3) == 0 && !__any_sync(FULL_MASK, live)) break;
+        const bool act = live && blk >= 0;
+        const int c = blk * TNS;
 
-        int vi[TN];
+        int vi[TNS];
 #pragma unroll
-        for (int j = 0; j < TN; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1, SEG);
+        for (int j = 0; j < TNS; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1, SEG);
         if (sl == 0) {
-            const int c = blk * TN;
 #pragma unroll
-            for (int j = 0; j < TN; ++j) vi[j] = (act && c + j < T.n) ? T.m + c + j : INT_MAX;
+            for (int j = 0; j < TNS; ++j) vi[j] = (act && c + j < T.n) ? T.m + c + j : INT_MAX;
         }
 
-        int bs[TN];
-        if (act) {
-            const int c = blk * TN;
-            if (c + TN <= T.n && (reinterpret_cast<uintptr_t>(T.b) & 3) == 0) {
+        int bs[TNS];
+        if (act && c + TNS <= T.n) {
+            if constexpr (TNS == 8) {
+                const uint2 w = __ldg(reinterpret_cast<const uint2 *>(T.b + c));
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    bs[j] = int((w.x >> (8 * j)) & 0xffu);
+                    bs[4 + j] = int((w.y >> (8 * j)) & 0xffu);
+                }
+            } else {
                 const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(T.b + c));
 #pragma unroll
-                for (int j = 0; j < TN; ++j) bs[j] = int((w >> (8 * j)) & 0xffu);
-            } else {
-#pragma unroll
-                for (int j = 0; j < TN; ++j) bs[j] = (c + j < T.n) ? int(__ldg(T.b + c + j)) : -2;
+                for (int j = 0; j < TNS; ++j) bs[j] = int((w >> (8 * j)) & 0xffu);
             }
         } else {
 #pragma unroll
-            for (int j = 0; j < TN; ++j) bs[j] = -2;
+            for (int j = 0; j < TNS; ++j) bs[j] = (act && c + j < T.n) ? int(__ldg(T.b + c + j)) : -2;
         }
 
 #pragma unroll
-        for (int j = 0; j < TN; ++j) {
+        for (int j = 0; j < TNS; ++j) {
             int v = vi[j];
 #pragma unroll
             for (int k = 0; k < TM; ++k) cell(av[k], bs[j], hv[k], v);
@@ -396,13 +396,12 @@ __device__ __forceinline__ void stream_segment(const BatchLaunch &B, int seg_id,
         }
 
         if (sl == SEG - 1 && act) {
-            const int c = blk * TN;
 #pragma unroll
-            for (int j = 0; j < TN; ++j)
+            for (int j = 0; j < TNS; ++j)
                 if (c + j < T.n) T.v_out[c + j] = vc[j];
         }
 
-        if (busy && ++blk == T.nb) {
+        if (live && ++blk == T.nb) {
             // This lane leaves pair q: write its h strands, move to pair q+1
             // (already fetched) and fetch pair q+2.
 #pragma unroll
@@ -410,26 +409,39 @@ __device__ __forceinline__ void stream_segment(const BatchLaunch &B, int seg_id,
                 if (r0 + k < T.m) T.h_out[T.m - 1 - r0 - k] = hv[k];
             ++q;
             take_next<TM>(L, N, r0, T, av, hv);
+            T.nb = (T.n + TNS - 1) / TNS;
             fetch_next<TM>(L, q + 1 < count ? list[q + 1] : -1, r0, N);
             blk = 0;
         }
     }
 }
 
-template <int TM, int SEG, int WARPS>
+// Stream classes compiled into the batch kernel: (rows per lane, lanes per segment).
+#define SLCS_STREAM_CLASSES(X) X(4, 8) X(4, 16) X(4, 32) X(8, 8) X(8, 16) X(8, 32) \
+    X(12, 8) X(12, 16) X(12, 32) X(16, 8) X(16, 16) X(16, 32)
+
+template <int TNS, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) comb_batch_kernel(const BatchLaunch B)
 {
     __shared__ __align__(16) int4 wf_ring[WARPS][RING];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
+    const int gw = blockIdx.x * WARPS + w;
     const CombLaunch &L = B.wf;
-    // Phase 1: this warp's stream segments (lists fixed by the plan).
-    if (B.nseg > 0) {
-        const int seg_id = (blockIdx.x * WARPS + w) * (32 / SEG) + lane / SEG;
-        stream_segment<TM, SEG>(B, seg_id, lane);
+    // Phase 1: this warp's stream segments (class and lists fixed by the plan).
+    if (gw < B.nwarps) {
+        int cls = 0;
+        while (cls < B.nclass - 1 && gw >= B.class_warp_end[cls]) ++cls;
+        const int code = B.class_code[cls];
+#define SLCS_CASE(TM, SEG)                                                                 \
+    case TM * 100 + SEG:                                                                   \
+        stream_segment<TM, SEG, TNS>(B, SEG_SLOTS * gw + lane / SEG, lane);                \
+        break;
+        switch (code) { SLCS_STREAM_CLASSES(SLCS_CASE) default: break; }
+#undef SLCS_CASE
     }
-    // Phase 2: stripes of multi-stripe pairs, whole warps, wavefront order,
-    // taken dynamically so that they also absorb the stream phase's tail.
+    // Phase 2: stripes of pairs too tall to stream, whole warps, wavefront
+    // order, taken dynamically so that they also absorb the stream tail.
     for (;;) {
         int k = 0;
         if (lane == 0) k = ld_relaxed_gpu(L.counters + 1) ? INT_MAX : atomicAdd(L.counters, 1);
@@ -478,7 +490,7 @@ slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_o
     return SLCS_OK;
 }
 
-template <int TM, int SEG, int WARPS>
+template <int TNS, int WARPS>
 slcs_status launch_batch_variant(const BatchLaunch &B, cudaStream_t stream, int *grid_out)
 {
     static int occ = -1;
@@ -486,8 +498,7 @@ slcs_status launch_batch_variant(const BatchLaunch &B, cudaStream_t stream, int 
     {
         std::lock_guard<std::mutex> g(mu);
         if (occ < 0) {
-            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_batch_kernel<TM, SEG, WARPS>,
-                                                                    WARPS * 32, 0));
+            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_batch_kernel<TNS, WARPS>, WARPS * 32, 0));
             if (occ < 1) occ = 1;
         }
     }
@@ -497,7 +508,7 @@ slcs_status launch_batch_variant(const BatchLaunch &B, cudaStream_t stream, int 
     }
     int grid = B.grid;
     if (grid < 1) grid = 1;
-    comb_batch_kernel<TM, SEG, WARPS><<<grid, WARPS * 32, 0, stream>>>(B);
+    comb_batch_kernel<TNS, WARPS><<<grid, WARPS * 32, 0, stream>>>(B);
     if (grid_out) *grid_out = grid;
     SLCS_CUDA(cudaGetLastError());
     return SLCS_OK;
@@ -555,23 +566,12 @@ bool stream_variant_supported(int tm, int seg)
     return (tm == 4 || tm == 8 || tm == 12 || tm == 16) && (seg == 8 || seg == 16 || seg == 32);
 }
 
-slcs_status launch_batch(const BatchLaunch &B, int tm, int seg, cudaStream_t stream, int *grid_out)
+slcs_status launch_batch(const BatchLaunch &B, int tns, cudaStream_t stream, int *grid_out)
 {
-    if (stream != PREPARE_ONLY && B.wf.ntasks <= 0 && B.nseg <= 0) return SLCS_OK;
-#define SLCS_SEG_CASE(TM)                                                               \
-    case TM:                                                                            \
-        if (seg == 8) return launch_batch_variant<TM, 8, BATCH_WARPS>(B, stream, grid_out);   \
-        if (seg == 16) return launch_batch_variant<TM, 16, BATCH_WARPS>(B, stream, grid_out); \
-        return launch_batch_variant<TM, 32, BATCH_WARPS>(B, stream, grid_out);
-    if (!stream_variant_supported(tm, seg)) return fail(SLCS_ERR_UNSUPPORTED, "stream tile_m/seg not supported");
-    switch (tm) {
-        SLCS_SEG_CASE(4)
-        SLCS_SEG_CASE(8)
-        SLCS_SEG_CASE(12)
-        SLCS_SEG_CASE(16)
-    }
-#undef SLCS_SEG_CASE
-    return fail(SLCS_ERR_UNSUPPORTED, "stream tile_m/seg not supported");
+    if (stream != PREPARE_ONLY && B.wf.ntasks <= 0 && B.nwarps <= 0) return SLCS_OK;
+    if (tns == 8) return launch_batch_variant<8, BATCH_WARPS>(B, stream, grid_out);
+    if (tns == 4) return launch_batch_variant<4, BATCH_WARPS>(B, stream, grid_out);
+    return fail(SLCS_ERR_UNSUPPORTED, "stream columns per step must be 4 or 8");
 }
 
 bool tile_m_supported(int tm) { return tm == 2 || tm == 4 || tm == 8 || tm == 12 || tm == 16; }

@@ -29,12 +29,17 @@ struct CombLaunch {
 // (whole warps, tile_m rows per lane), then every single-stripe pair is
 // streamed: a segment of `seg` lanes combs pair after pair without draining
 // its pipeline between them.
+constexpr int MAX_CLASSES = 6;
+constexpr int SEG_SLOTS = 4; // segment slots per warp (32 / smallest SEG)
 struct BatchLaunch {
-    CombLaunch wf;           // wavefront part (tasks of multi-stripe pairs)
-    const int32_t *seg_off;  // device: nseg+1 offsets into seg_list (CSR)
+    CombLaunch wf;           // wavefront part (tasks of pairs too tall to stream)
+    const int32_t *seg_off;  // device: SEG_SLOTS*nwarps+1 offsets into seg_list (CSR)
     const int32_t *seg_list; // device: pairs of each stream segment, in order
-    int32_t nseg;            // stream segments with a list (may be 0)
+    int32_t nwarps;          // warps 0..nwarps-1 (grid order) stream; the rest only take wavefront tasks
     int32_t grid;            // blocks of the persistent launch
+    int32_t nclass;          // stream classes; warp w serves the first class c with w < class_warp_end[c]
+    int32_t class_warp_end[MAX_CLASSES];
+    int32_t class_code[MAX_CLASSES]; // rows per lane * 100 + lanes per segment
 };
 
 // Rows of a one lane keeps in registers; supported values.
@@ -61,9 +66,10 @@ slcs_status launch_comb_on(const CombLaunch &L, int tile_m, int warps, int sms, 
 // Stream-mode variants: rows per lane and lanes per segment.
 bool stream_variant_supported(int stream_tm, int seg);
 // Enqueue one persistent batch launch (counters [0] wavefront ticket and [1]
-// abort must be zero).  Wavefront tasks use tile_m 8.  With PREPARE_ONLY as
-// the stream, *grid_out receives the full persistent grid (blocks).
-slcs_status launch_batch(const BatchLaunch &L, int stream_tm, int seg, cudaStream_t stream, int *grid_out);
+// abort must be zero).  Wavefront tasks use tile_m 8; streamed pairs advance
+// `tns` (4 or 8) columns per step.  With PREPARE_ONLY as the stream,
+// *grid_out receives the full persistent grid (blocks).
+slcs_status launch_batch(const BatchLaunch &L, int tns, cudaStream_t stream, int *grid_out);
 constexpr int BATCH_WARPS = 4;
 constexpr int BATCH_WF_TM = 8;
 

@@ -30,7 +30,7 @@ class Config(ctypes.Structure):
     _fields_ = [("algo", ctypes.c_int32), ("tile_m", ctypes.c_int32), ("tile_n", ctypes.c_int32),
                 ("warps", ctypes.c_int32), ("braid_cutoff", ctypes.c_int32), ("strips", ctypes.c_int32),
                 ("use_graph", ctypes.c_int32), ("seg", ctypes.c_int32), ("wait_ms", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 7)]
+                ("blocks_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
 
     @classmethod
     def make(cls, **kw) -> "Config":
@@ -49,7 +49,8 @@ class PairDesc(ctypes.Structure):
 class PlanInfo(ctypes.Structure):
     _fields_ = [("stream_tile_m", ctypes.c_int32), ("seg", ctypes.c_int32), ("wavefront_tile_m", ctypes.c_int32),
                 ("warps", ctypes.c_int32), ("stream_pairs", ctypes.c_int32), ("wavefront_tasks", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 2)]
+                ("stream_classes", ctypes.c_int32), ("tile_n", ctypes.c_int32), ("grid", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 3)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}

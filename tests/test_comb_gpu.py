@@ -108,14 +108,16 @@ def _batch_expected(batch):
     return O.comb_batch(batch.a_blob, batch.b_blob, batch.a_off, batch.b_off, batch.ms, batch.ns, off, total)
 
 
-@pytest.mark.parametrize("graph", [0, 1])
-def test_batch_reads(cuda, graph):
+@pytest.mark.parametrize("graph,tns,bpsm", [(0, 8, 0), (1, 8, 0), (0, 4, 0), (1, 8, 1), (0, 4, 2)])
+def test_batch_reads(cuda, graph, tns, bpsm):
+    """Default multi-class stream plan (every pair in the smallest row class)."""
     import torch
     batch = W.reads_20000(npairs=3000)
     descs = slcs.pair_descs(batch)
     _, total = batch.strand_offsets()
     out = torch.empty(total, dtype=torch.int32, device=cuda)
-    plan = slcs.BatchPlan(descs, slcs.Config.make(use_graph=graph))
+    plan = slcs.BatchPlan(descs, slcs.Config.make(use_graph=graph, tile_n=tns, blocks_per_sm=bpsm))
+    assert plan.info["stream_classes"] >= 3 and plan.info["tile_n"] == tns
     a_d, b_d = _dev(batch.a_blob, cuda), _dev(batch.b_blob, cuda)
     want = _batch_expected(batch)
     for _ in range(2):
@@ -152,15 +154,16 @@ def test_batch_mixed_sizes_wavefront(cuda):
     np.testing.assert_array_equal(host, want)
 
 
-@pytest.mark.parametrize("stm,seg", [(4, 8), (4, 32), (8, 16), (12, 16), (16, 8), (16, 16), (16, 32)])
-def test_batch_stream_variants(cuda, stm, seg):
+@pytest.mark.parametrize("stm,seg,tns", [(4, 8, 4), (4, 32, 8), (8, 16, 4), (12, 16, 8), (16, 8, 8), (16, 16, 4),
+                                         (16, 32, 8)])
+def test_batch_stream_variants(cuda, stm, seg, tns):
     """Stream mode (pairs of at most seg*stm rows) plus wavefront tasks for the rest."""
     import torch
     batch = _mixed_batch(20 + stm + seg, count=400, mmax=700, nmax=900)
     descs = slcs.pair_descs(batch)
     _, total = batch.strand_offsets()
     want = _batch_expected(batch)
-    plan = slcs.BatchPlan(descs, slcs.Config.make(tile_m=stm, seg=seg))
+    plan = slcs.BatchPlan(descs, slcs.Config.make(tile_m=stm, seg=seg, tile_n=tns))
     info = plan.info
     assert info["stream_tile_m"] == stm and info["seg"] == seg and info["stream_pairs"] > 0
     out = torch.full((total,), -7, dtype=torch.int32, device=cuda)
