@@ -66,7 +66,9 @@ typedef struct {
     int32_t seg;           /* batch stream mode: lanes per pipeline segment (8/16/32) */
     int32_t wait_ms;       /* limit of one device-side wait (default 10000 ms)        */
     int32_t blocks_per_sm; /* batch plans: resident blocks per SM (default: occupancy) */
-    int32_t reserved[6];
+    int32_t strand_bits;   /* batch plans: 16 = combine two pairs per register where ids fit 15 bits,
+                              32 = 32-bit strands only, 0 = engine default                 */
+    int32_t reserved[5];
 } slcs_config;
 
 /* One pair of a batch: symbols at a_blob[a_offset .. +m) and b_blob[b_offset .. +n);
@@ -169,7 +171,8 @@ typedef struct {
     int32_t stream_classes;  /* stream classes in use                               */
     int32_t tile_n;          /* stream columns per step                             */
     int32_t grid;            /* blocks of the launch                                */
-    int32_t reserved[3];
+    int32_t packed_pairs;    /* stream pairs combed two per register (16-bit ids)   */
+    int32_t reserved[2];
 } slcs_plan_info;
 SLCS_API slcs_status slcs_batch_plan_info(const slcs_batch_plan *plan, slcs_plan_info *info);
 

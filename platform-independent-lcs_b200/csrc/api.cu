@@ -162,6 +162,11 @@ static slcs_status write_identity(int32_t *h, int32_t m, int32_t *v, int32_t n, 
 
 using namespace slcs;
 
+struct StreamClass {
+    int tm, seg;
+    bool packed;
+};
+
 struct slcs_batch_plan {
     int device = 0;
     int tm = 8;      // rows per lane of the wavefront tasks
@@ -171,9 +176,10 @@ struct slcs_batch_plan {
     int32_t npairs = 0;
     int32_t ntasks = 0;
     int32_t nstream = 0;
+    int32_t npacked = 0; // stream pairs in packed classes
     int tns = 8;        // stream columns per step
     int blocks_per_sm = 0;
-    std::vector<std::pair<int, int>> classes; // stream classes (rows per lane, lanes per segment)
+    std::vector<StreamClass> classes; // stream classes in preference order
     int32_t nclass = 0; // classes with warps
     int32_t class_warp_end[MAX_CLASSES] = {};
     int32_t class_code[MAX_CLASSES] = {};
@@ -184,6 +190,7 @@ struct slcs_batch_plan {
     PairDev *d_pairs = nullptr;
     int32_t *d_seg_off = nullptr;
     int32_t *d_seg_list = nullptr;
+    int32_t *d_seg_list2 = nullptr;
     int2 *d_tasks = nullptr;
     int64_t *d_scr_off = nullptr;
     int32_t *d_scratch = nullptr;
@@ -222,7 +229,7 @@ struct slcs_batch_plan {
         SLCS_CUDA(cudaMemsetAsync(d_work, 0, work_bytes, st));
         slcs_status s;
         if (stm > 0) {
-            BatchLaunch B{launch(a, b, out), d_seg_off, d_seg_list, nwarps, grid, nclass, {}, {}};
+            BatchLaunch B{launch(a, b, out), d_seg_off, d_seg_list, d_seg_list2, nwarps, grid, nclass, {}, {}};
             for (int c = 0; c < nclass; ++c) {
                 B.class_warp_end[c] = class_warp_end[c];
                 B.class_code[c] = class_code[c];
@@ -431,22 +438,37 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
         // taller pairs run as wavefront tasks of BATCH_WF_TM rows per lane.
         // A configuration naming tile_m (and seg) asks for that one class.
         P->tm = BATCH_WF_TM;
-        P->tns = (cfg && cfg->tile_n) ? cfg->tile_n : 8;
+        const int bits = cfg ? cfg->strand_bits : 0;
+        if (bits != 0 && bits != 16 && bits != 32) {
+            delete P;
+            return fail(SLCS_ERR_UNSUPPORTED, "strand_bits must be 0, 16 or 32");
+        }
+        // Two pairs per register (4 columns per step) when some pair fits a
+        // packed class; otherwise 8 columns per step by default.
+        bool packable = false;
+        for (int32_t p = 0; p < npairs && !packable; ++p)
+            packable = pairs[p].m > 0 && pairs[p].m <= 256 && int64_t(pairs[p].m) + pairs[p].n <= PACKED16_MAX_IDS;
+        P->tns = (cfg && cfg->tile_n) ? cfg->tile_n : (bits != 32 && packable ? 4 : 8);
         if (P->tns != 4 && P->tns != 8) {
             delete P;
             return fail(SLCS_ERR_UNSUPPORTED, "stream mode needs tile_n 4 or 8");
         }
+        const bool pack = bits != 32 && P->tns == 4;
         if (cfg && cfg->tile_m) {
             P->stm = cfg->tile_m;
             P->seg = cfg->seg ? cfg->seg : 16;
-            P->classes = {{P->stm, P->seg}};
+            if (pack && packed16_supported(P->stm, P->seg)) P->classes.push_back({P->stm, P->seg, true});
+            P->classes.push_back({P->stm, P->seg, false});
         } else {
             P->stm = 16;
             P->seg = 16;
-            P->classes = {{4, 16}, {8, 16}, {12, 16}, {16, 16}, {16, 32}};
+            if (pack)
+                for (int t : {4, 8, 12, 16}) P->classes.push_back({t, 16, true});
+            for (int t : {4, 8, 12, 16}) P->classes.push_back({t, 16, false});
+            P->classes.push_back({16, 32, false});
         }
         for (const auto &c : P->classes)
-            if (!stream_variant_supported(c.first, c.second)) {
+            if (!stream_variant_supported(c.tm, c.seg)) {
                 delete P;
                 return fail(SLCS_ERR_UNSUPPORTED, "stream mode needs tile_m in {4,8,12,16} and seg in {8,16,32}");
             }
@@ -459,7 +481,7 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
         P->need_out = std::max<int64_t>(P->need_out, pairs[p].out_offset + pairs[p].m + pairs[p].n);
     }
     int32_t stream_rows = 0;
-    for (const auto &c : P->classes) stream_rows = std::max(stream_rows, c.first * c.second);
+    for (const auto &c : P->classes) stream_rows = std::max(stream_rows, c.tm * c.seg);
     Schedule S = build_schedule(pairs, npairs, P->tm, stream_rows);
     P->ntasks = int32_t(S.tasks.size());
     // One-time device set-up now, so a graph capture in run() issues only
@@ -482,27 +504,47 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
     // warp (a warp runs 32/seg segments side by side), and within a class
     // the pairs go longest first to the least loaded segment.  The grid is
     // the persistent one (or blocks_per_sm per SM), fewer for small batches.
-    std::vector<int32_t> seg_off, seg_list;
+    std::vector<int32_t> seg_off, seg_list, seg_list2;
     if (P->stm > 0) {
         const int occ_blocks = std::max(1, full_grid / std::max(1, sm_count()));
         int grid = sm_count() * (P->blocks_per_sm > 0 ? std::min(P->blocks_per_sm, occ_blocks) : occ_blocks);
         const int nclass = int(P->classes.size());
+        // Items of a class: single pairs, or couples (pair A, pair B) for a
+        // packed class -- its pairs sorted by length and taken two by two.
         std::vector<std::vector<int32_t>> cls_pairs(nclass);
         for (int32_t p : S.stream_pairs) { // largest first
             int c = 0;
-            while (c < nclass - 1 && pairs[p].m > P->classes[c].first * P->classes[c].second) ++c;
-            cls_pairs[c].push_back(p);
+            for (; c < nclass; ++c) {
+                const StreamClass &k = P->classes[c];
+                if (pairs[p].m <= k.tm * k.seg && (!k.packed || int64_t(pairs[p].m) + pairs[p].n <= PACKED16_MAX_IDS))
+                    break;
+            }
+            cls_pairs[std::min(c, nclass - 1)].push_back(p);
         }
-        auto cost = [&](int32_t p) { return int64_t((pairs[p].n + P->tns - 1) / P->tns) + 2; };
+        std::vector<std::vector<std::pair<int32_t, int32_t>>> items(nclass);
+        for (int c = 0; c < nclass; ++c) {
+            auto &cp = cls_pairs[c];
+            if (P->classes[c].packed) {
+                std::stable_sort(cp.begin(), cp.end(), [&](int32_t x, int32_t y) { return pairs[x].n > pairs[y].n; });
+                for (size_t i = 0; i < cp.size(); i += 2)
+                    items[c].push_back({cp[i], i + 1 < cp.size() ? cp[i + 1] : -1});
+            } else {
+                for (int32_t p : cp) items[c].push_back({p, -1});
+            }
+        }
+        auto cost = [&](const std::pair<int32_t, int32_t> &it) {
+            const int32_t n = std::max(pairs[it.first].n, it.second >= 0 ? pairs[it.second].n : 0);
+            return int64_t((n + P->tns - 1) / P->tns) + 2;
+        };
         std::vector<double> wsteps(nclass, 0.0);
         std::vector<long> wmax(nclass, 0);
         double total = 0.0;
         for (int c = 0; c < nclass; ++c) {
             int64_t w = 0;
-            for (int32_t p : cls_pairs[c]) w += cost(p);
-            const int spw = 32 / P->classes[c].second;
+            for (const auto &it : items[c]) w += cost(it);
+            const int spw = 32 / P->classes[c].seg;
             wsteps[c] = double(w) / spw;
-            wmax[c] = (long(cls_pairs[c].size()) + spw - 1) / spw;
+            wmax[c] = (long(items[c].size()) + spw - 1) / spw;
             total += wsteps[c];
         }
         const long want_wf = (long(P->ntasks) + BATCH_WARPS - 1) / BATCH_WARPS;
@@ -515,7 +557,7 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
         std::vector<long> wc(nclass, 0);
         long used = 0;
         for (int c = 0; c < nclass; ++c) {
-            if (cls_pairs[c].empty()) continue;
+            if (items[c].empty()) continue;
             long w = total > 0 ? long(double(warps_total) * wsteps[c] / total) : 1;
             w = std::max(1L, std::min(w, wmax[c]));
             wc[c] = w;
@@ -527,28 +569,38 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
             --wc[big];
             --used;
         }
+        if (std::count_if(wc.begin(), wc.end(), [](long w) { return w > 0; }) > MAX_CLASSES) {
+            delete P;
+            return fail(SLCS_ERR_UNSUPPORTED, "too many stream classes in use");
+        }
         P->grid = int(std::max<long>(grid, (used + BATCH_WARPS - 1) / BATCH_WARPS));
         P->nclass = 0;
         long wbase = 0;
-        std::vector<std::vector<int32_t>> slot_lists(size_t(std::max(used, 1L)) * SEG_SLOTS);
+        std::vector<std::vector<std::pair<int32_t, int32_t>>> slot_lists(size_t(std::max(used, 1L)) * SEG_SLOTS);
         for (int c = 0; c < nclass; ++c) {
             if (wc[c] == 0) continue;
-            const int spw = 32 / P->classes[c].second;
+            const int spw = 32 / P->classes[c].seg;
             const long nseg = wc[c] * spw;
             using Load = std::pair<int64_t, int64_t>;
             std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
             for (long sgi = 0; sgi < nseg; ++sgi) heap.push({0, sgi});
-            for (int32_t p : cls_pairs[c]) {
+            std::stable_sort(items[c].begin(), items[c].end(),
+                             [&](const std::pair<int32_t, int32_t> &x, const std::pair<int32_t, int32_t> &y) {
+                                 return cost(x) > cost(y);
+                             });
+            for (const auto &it : items[c]) {
                 Load top = heap.top();
                 heap.pop();
-                const long warp = wbase + top.second / spw, s = top.second % spw;
-                slot_lists[size_t(warp) * SEG_SLOTS + size_t(s)].push_back(p);
-                top.first += cost(p);
+                const long warp = wbase + top.second / spw, sidx = top.second % spw;
+                slot_lists[size_t(warp) * SEG_SLOTS + size_t(sidx)].push_back(it);
+                top.first += cost(it);
                 heap.push(top);
             }
             wbase += wc[c];
+            if (P->classes[c].packed) P->npacked += int32_t(cls_pairs[c].size());
             P->class_warp_end[P->nclass] = int32_t(wbase);
-            P->class_code[P->nclass] = P->classes[c].first * 100 + P->classes[c].second;
+            P->class_code[P->nclass] = P->classes[c].tm * 100 + P->classes[c].seg +
+                                       (P->classes[c].packed ? PACKED16_CODE : 0);
             ++P->nclass;
         }
         P->nwarps = int32_t(wbase);
@@ -556,7 +608,10 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
             seg_off.reserve(size_t(P->nwarps) * SEG_SLOTS + 1);
             seg_off.push_back(0);
             for (long sl = 0; sl < long(P->nwarps) * SEG_SLOTS; ++sl) {
-                seg_list.insert(seg_list.end(), slot_lists[size_t(sl)].begin(), slot_lists[size_t(sl)].end());
+                for (const auto &it : slot_lists[size_t(sl)]) {
+                    seg_list.push_back(it.first);
+                    seg_list2.push_back(it.second);
+                }
                 seg_off.push_back(int32_t(seg_list.size()));
             }
         }
@@ -569,6 +624,9 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
     alloc(reinterpret_cast<void **>(&P->d_pairs), sizeof(PairDev) * size_t(npairs));
     alloc(reinterpret_cast<void **>(&P->d_seg_off), sizeof(int32_t) * seg_off.size());
     alloc(reinterpret_cast<void **>(&P->d_seg_list), sizeof(int32_t) * seg_list.size());
+    alloc(reinterpret_cast<void **>(&P->d_seg_list2), sizeof(int32_t) * seg_list2.size());
+    if (e == cudaSuccess && !seg_list2.empty())
+        e = cudaMemcpy(P->d_seg_list2, seg_list2.data(), sizeof(int32_t) * seg_list2.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !seg_off.empty())
         e = cudaMemcpy(P->d_seg_off, seg_off.data(), sizeof(int32_t) * seg_off.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !seg_list.empty())
@@ -604,6 +662,7 @@ slcs_status slcs_batch_plan_info(const slcs_batch_plan *P, slcs_plan_info *info)
     info->warps = P->warps;
     info->stream_pairs = P->nstream;
     info->wavefront_tasks = P->ntasks;
+    info->packed_pairs = P->npacked;
     return SLCS_OK;
 }
 
@@ -686,6 +745,7 @@ slcs_status slcs_batch_plan_destroy(slcs_batch_plan *P)
     cudaFree(P->d_pairs);
     cudaFree(P->d_seg_off);
     cudaFree(P->d_seg_list);
+    cudaFree(P->d_seg_list2);
     cudaFree(P->d_tasks);
     cudaFree(P->d_scr_off);
     cudaFree(P->d_scratch);

@@ -369,7 +369,8 @@ __device__ __forceinline__ void stream_segment(const BatchLaunch &B, int seg_id,
         }
 
         int bs[TNS];
-        if (act && c + TNS <= T.n) {
+        // Whole-word loads only where b is aligned to TNS bytes (c is a multiple of TNS).
+        if (act && c + TNS <= T.n && (reinterpret_cast<uintptr_t>(T.b) & (TNS - 1)) == 0) {
             if constexpr (TNS == 8) {
                 const uint2 w = __ldg(reinterpret_cast<const uint2 *>(T.b + c));
 #pragma unroll
@@ -416,9 +417,187 @@ __device__ __forceinline__ void stream_segment(const BatchLaunch &B, int seg_id,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Packed stream mode: two pairs per register.
+//
+// A couple of pairs (A, B) of one row class is combed together: every symbol,
+// h and v register holds pair A in its low 16 bits and pair B in its high 16
+// bits, so one instruction works on two cells.  Strand ids are stored plus
+// one (1..32767); a masked row holds h = 0 and symbol 0x1FF, a masked column
+// v = 0x7FFF and symbol 0x100, so neither ever swaps.  The cell rule per half
+// is evaluated in bit 15 without carries between the halves:
+//   y = (a ^ b) + 0x7FFF      bit 15 set iff the symbols differ (a^b <= 0x1FF)
+//   d = (v + 0x8000) - h      bit 15 set iff v >= h (no crossing)
+//   keep = d & y & 0x8000 -> expanded to 0xFFFF by a sign-replicating byte
+//   permute (PTX prmt with selector nibbles 0x9/0xB: bit 3 of a nibble
+//   replicates the sign of the chosen byte; __byte_perm only copies bytes);
+//   h' = keep ? h : v, v' = keep ? v : h.
+// Both pairs of a couple switch together after max(nb_A, nb_B) blocks; the
+// shorter pair's extra columns are masked.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cell16(uint32_t a, uint32_t b, uint32_t &h, uint32_t &v)
+{
+    const uint32_t y = (a ^ b) + 0x7FFF7FFFu;
+    const uint32_t d = (v + 0x80008000u) - h;
+    uint32_t keep;
+    asm("prmt.b32 %0, %1, 0, 0xBB99;" : "=r"(keep) : "r"(d & y & 0x80008000u));
+    const uint32_t nh = (h & keep) | (v & ~keep);
+    v = (v & keep) | (h & ~keep);
+    h = nh;
+}
+
+template <int TM>
+struct CoupleTask {
+    int pa, pb;      // pair indices (-1: none)
+    int ma, na, mb, nb_cols, nb;
+    const uint8_t *ba, *bb;
+    int32_t *ha, *va, *hb, *vb;
+};
+
+template <int TM>
+struct NextCouple {
+    NextPair<TM> A, B;
+};
+
+// Make a fetched couple current: packed row symbols and start ids.
+template <int TM>
+__device__ __forceinline__ void take_couple(const CombLaunch &L, const NextCouple<TM> &N, int r0, CoupleTask<TM> &T,
+                                            uint32_t (&ap)[TM], uint32_t (&hp)[TM])
+{
+    StreamTask<TM> A, B;
+    int aa[TM], ha[TM], ab[TM], hb[TM];
+    take_next<TM>(L, N.A, r0, A, aa, ha);
+    take_next<TM>(L, N.B, r0, B, ab, hb);
+    T.pa = A.pair;
+    T.pb = B.pair;
+    T.ma = A.m;
+    T.na = A.n;
+    T.mb = B.m;
+    T.nb_cols = B.n;
+    T.ba = A.b;
+    T.bb = B.b;
+    T.ha = A.h_out;
+    T.va = A.v_out;
+    T.hb = B.h_out;
+    T.vb = B.v_out;
+    T.nb = (max(A.n, B.n) + 3) / 4;
+#pragma unroll
+    for (int k = 0; k < TM; ++k) {
+        const uint32_t lo = aa[k] < 0 ? 0x1FFu : uint32_t(aa[k]);
+        const uint32_t hi = ab[k] < 0 ? 0x1FFu : uint32_t(ab[k]);
+        ap[k] = lo | (hi << 16);
+        const uint32_t hl = ha[k] < 0 ? 0u : uint32_t(ha[k] + 1);
+        const uint32_t hh = hb[k] < 0 ? 0u : uint32_t(hb[k] + 1);
+        hp[k] = hl | (hh << 16);
+    }
+}
+
+// Four symbols of one pair at columns c..c+3 as bytes (masked: 0x100 later).
+__device__ __forceinline__ uint32_t sym4(const uint8_t *b, int c, int n, bool &full)
+{
+    full = c + 4 <= n;
+    if (full && (reinterpret_cast<uintptr_t>(b + c) & 3) == 0) return __ldg(reinterpret_cast<const uint32_t *>(b + c));
+    uint32_t w = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (c + j < n) w |= uint32_t(__ldg(b + c + j)) << (8 * j);
+    full = false;
+    return w;
+}
+
+template <int TM, int SEG>
+__device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int seg_id, int lane)
+{
+    const CombLaunch &L = B.wf;
+    const int sl = lane & (SEG - 1);
+    const int r0 = sl * TM;
+    const int beg = B.seg_off[seg_id];
+    const int32_t *la = B.seg_list + beg;
+    const int32_t *lb = B.seg_list2 + beg;
+    const int count = B.seg_off[seg_id + 1] - beg;
+
+    int q = 0;
+    CoupleTask<TM> T;
+    NextCouple<TM> N;
+    uint32_t ap[TM], hp[TM];
+    fetch_next<TM>(L, count > 0 ? la[0] : -1, r0, N.A);
+    fetch_next<TM>(L, count > 0 ? lb[0] : -1, r0, N.B);
+    take_couple<TM>(L, N, r0, T, ap, hp);
+    fetch_next<TM>(L, count > 1 ? la[1] : -1, r0, N.A);
+    fetch_next<TM>(L, count > 1 ? lb[1] : -1, r0, N.B);
+    int blk = -sl;
+
+    uint32_t vc[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) vc[j] = 0x7FFF7FFFu;
+
+    for (int it = 0;; ++it) {
+        const bool live = T.pa >= 0;
+        if ((it & 3) == 0 && !__any_sync(FULL_MASK, live)) break;
+        const bool act = live && blk >= 0;
+        const int c = blk * 4;
+
+        uint32_t vi[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1, SEG);
+        if (sl == 0) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t lo = (act && c + j < T.na) ? uint32_t(T.ma + c + j + 1) : 0x7FFFu;
+                const uint32_t hi = (act && T.pb >= 0 && c + j < T.nb_cols) ? uint32_t(T.mb + c + j + 1) : 0x7FFFu;
+                vi[j] = lo | (hi << 16);
+            }
+        }
+
+        uint32_t bp[4];
+        {
+            bool fa = false, fb = false;
+            const uint32_t wa = act ? sym4(T.ba, c, T.na, fa) : 0u;
+            const uint32_t wb = (act && T.pb >= 0) ? sym4(T.bb, c, T.nb_cols, fb) : 0u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t sa = (act && c + j < T.na) ? ((wa >> (8 * j)) & 0xffu) : 0x100u;
+                const uint32_t sb = (act && T.pb >= 0 && c + j < T.nb_cols) ? ((wb >> (8 * j)) & 0xffu) : 0x100u;
+                bp[j] = sa | (sb << 16);
+            }
+        }
+
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            uint32_t v = vi[j];
+#pragma unroll
+            for (int k = 0; k < TM; ++k) cell16(ap[k], bp[j], hp[k], v);
+            vc[j] = v;
+        }
+
+        if (sl == SEG - 1 && act) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (c + j < T.na) T.va[c + j] = int32_t(vc[j] & 0xFFFFu) - 1;
+                if (T.pb >= 0 && c + j < T.nb_cols) T.vb[c + j] = int32_t(vc[j] >> 16) - 1;
+            }
+        }
+
+        if (live && ++blk == T.nb) {
+#pragma unroll
+            for (int k = 0; k < TM; ++k) {
+                if (r0 + k < T.ma) T.ha[T.ma - 1 - r0 - k] = int32_t(hp[k] & 0xFFFFu) - 1;
+                if (T.pb >= 0 && r0 + k < T.mb) T.hb[T.mb - 1 - r0 - k] = int32_t(hp[k] >> 16) - 1;
+            }
+            ++q;
+            take_couple<TM>(L, N, r0, T, ap, hp);
+            fetch_next<TM>(L, (T.pa >= 0 && q + 1 < count) ? la[q + 1] : -1, r0, N.A);
+            fetch_next<TM>(L, (T.pa >= 0 && q + 1 < count) ? lb[q + 1] : -1, r0, N.B);
+            blk = 0;
+        }
+    }
+}
+
 // Stream classes compiled into the batch kernel: (rows per lane, lanes per segment).
 #define SLCS_STREAM_CLASSES(X) X(4, 8) X(4, 16) X(4, 32) X(8, 8) X(8, 16) X(8, 32) \
     X(12, 8) X(12, 16) X(12, 32) X(16, 8) X(16, 16) X(16, 32)
+// Packed classes (4 columns per step).
+#define SLCS_PACKED_CLASSES(X) X(4, 16) X(8, 16) X(12, 16) X(16, 16)
 
 template <int TNS, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) comb_batch_kernel(const BatchLaunch B)
@@ -439,6 +618,14 @@ __global__ void __launch_bounds__(WARPS * 32) comb_batch_kernel(const BatchLaunc
         break;
         switch (code) { SLCS_STREAM_CLASSES(SLCS_CASE) default: break; }
 #undef SLCS_CASE
+        if (TNS == 4) {
+#define SLCS_PCASE(TM, SEG)                                                                \
+    case PACKED16_CODE + TM * 100 + SEG:                                                   \
+        stream_segment16<TM, SEG>(B, SEG_SLOTS * gw + lane / SEG, lane);                   \
+        break;
+            switch (code) { SLCS_PACKED_CLASSES(SLCS_PCASE) default: break; }
+#undef SLCS_PCASE
+        }
     }
     // Phase 2: stripes of pairs too tall to stream, whole warps, wavefront
     // order, taken dynamically so that they also absorb the stream tail.
@@ -560,6 +747,8 @@ slcs_status launch_comb_on(const CombLaunch &L, int tile_m, int warps, int sms, 
     }
 #undef SLCS_TM_ON
 }
+
+bool packed16_supported(int tm, int seg) { return (tm == 4 || tm == 8 || tm == 12 || tm == 16) && seg == 16; }
 
 bool stream_variant_supported(int tm, int seg)
 {

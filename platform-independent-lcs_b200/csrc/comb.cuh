@@ -29,18 +29,24 @@ struct CombLaunch {
 // (whole warps, tile_m rows per lane), then every single-stripe pair is
 // streamed: a segment of `seg` lanes combs pair after pair without draining
 // its pipeline between them.
-constexpr int MAX_CLASSES = 6;
+constexpr int MAX_CLASSES = 10;
 constexpr int SEG_SLOTS = 4; // segment slots per warp (32 / smallest SEG)
 struct BatchLaunch {
     CombLaunch wf;           // wavefront part (tasks of pairs too tall to stream)
     const int32_t *seg_off;  // device: SEG_SLOTS*nwarps+1 offsets into seg_list (CSR)
     const int32_t *seg_list; // device: pairs of each stream segment, in order
+    const int32_t *seg_list2; // device: packed classes: the partner pair combed in the high half (-1: none)
     int32_t nwarps;          // warps 0..nwarps-1 (grid order) stream; the rest only take wavefront tasks
     int32_t grid;            // blocks of the persistent launch
     int32_t nclass;          // stream classes; warp w serves the first class c with w < class_warp_end[c]
     int32_t class_warp_end[MAX_CLASSES];
-    int32_t class_code[MAX_CLASSES]; // rows per lane * 100 + lanes per segment
+    int32_t class_code[MAX_CLASSES]; // rows per lane * 100 + lanes per segment (+ PACKED16_CODE when packed)
 };
+// Class-code offset of the packed variant: two pairs per register, strand ids
+// in 15 bits (pairs with m + n <= PACKED16_MAX_IDS), 4 columns per step.
+constexpr int PACKED16_CODE = 10000;
+constexpr int PACKED16_MAX_IDS = 32767;
+bool packed16_supported(int tm, int seg);
 
 // Rows of a one lane keeps in registers; supported values.
 bool tile_m_supported(int tm);

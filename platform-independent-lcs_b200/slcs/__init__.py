@@ -30,7 +30,8 @@ class Config(ctypes.Structure):
     _fields_ = [("algo", ctypes.c_int32), ("tile_m", ctypes.c_int32), ("tile_n", ctypes.c_int32),
                 ("warps", ctypes.c_int32), ("braid_cutoff", ctypes.c_int32), ("strips", ctypes.c_int32),
                 ("use_graph", ctypes.c_int32), ("seg", ctypes.c_int32), ("wait_ms", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
+                ("blocks_per_sm", ctypes.c_int32), ("strand_bits", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 5)]
 
     @classmethod
     def make(cls, **kw) -> "Config":
@@ -50,7 +51,7 @@ class PlanInfo(ctypes.Structure):
     _fields_ = [("stream_tile_m", ctypes.c_int32), ("seg", ctypes.c_int32), ("wavefront_tile_m", ctypes.c_int32),
                 ("warps", ctypes.c_int32), ("stream_pairs", ctypes.c_int32), ("wavefront_tasks", ctypes.c_int32),
                 ("stream_classes", ctypes.c_int32), ("tile_n", ctypes.c_int32), ("grid", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 3)]
+                ("packed_pairs", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}

@@ -188,3 +188,142 @@ def test_batch_stream_tiny_pairs(cuda):
         plan.run(_dev(batch.a_blob, cuda), _dev(batch.b_blob, cuda), out)
         torch.cuda.synchronize()
         np.testing.assert_array_equal(out.cpu().numpy(), _batch_expected(batch))
+
+
+def _pack_unaligned(pairs, seed):
+    """Like workloads.pack, but every string starts at a random byte offset."""
+    rng = np.random.default_rng(seed)
+
+    def blob(strings):
+        off = np.zeros(len(strings), np.int64)
+        pos = 0
+        for i, s in enumerate(strings):
+            pos += int(rng.integers(0, 4))
+            off[i] = pos
+            pos += len(s)
+        buf = np.zeros(pos + 16, np.uint8)
+        for o, s in zip(off, strings):
+            buf[o:o + len(s)] = s
+        return buf, off
+
+    a_blob, a_off = blob([a for a, _ in pairs])
+    b_blob, b_off = blob([b for _, b in pairs])
+    return W.Batch(a_blob, b_blob, a_off, b_off, np.array([len(a) for a, _ in pairs], np.int32),
+                   np.array([len(b) for _, b in pairs], np.int32))
+
+
+def _run_plan(batch, cfg, cuda):
+    import torch
+    descs = slcs.pair_descs(batch)
+    _, total = batch.strand_offsets()
+    plan = slcs.BatchPlan(descs, cfg)
+    out = torch.full((total,), -7, dtype=torch.int32, device=cuda)
+    plan.run(_dev(batch.a_blob, cuda), _dev(batch.b_blob, cuda), out)
+    torch.cuda.synchronize()
+    slcs.device_status(0)
+    info = plan.info
+    plan.close()
+    return out.cpu().numpy(), info
+
+
+def test_batch_packed_reads_match_32bit(cuda):
+    """Default plan on read pairs combs two pairs per register; forcing 32-bit
+    strands gives the same strands."""
+    batch = W.reads_20000(npairs=2001)
+    want = _batch_expected(batch)
+    got, info = _run_plan(batch, slcs.Config.make(), cuda)
+    assert info["packed_pairs"] > 1000 and info["tile_n"] == 4
+    np.testing.assert_array_equal(got, want)
+    got32, info32 = _run_plan(batch, slcs.Config.make(strand_bits=32), cuda)
+    assert info32["packed_pairs"] == 0
+    np.testing.assert_array_equal(got32, want)
+
+
+def _packed_class_pairs(stm):
+    rng = np.random.default_rng(300 + stm)
+    rows = 16 * stm
+    pairs = []
+    for i in range(161):
+        m = int(rng.integers(1, rows + 1))
+        n = int(rng.integers(1, 700))
+        if i % 40 == 0:
+            n = 32767 - m
+        elif i % 40 == 1:
+            n = 32768 - m
+        elif i % 53 == 5:
+            n = 0
+        sigma = int(rng.choice([2, 4, 20, 256]))
+        pairs.append((rng.integers(0, sigma, m, dtype=np.uint8), rng.integers(0, sigma, n, dtype=np.uint8)))
+    return pairs
+
+
+@pytest.mark.parametrize("stm", [4, 8, 12, 16])
+def test_batch_packed_classes(cuda, stm):
+    """One packed class plus its 32-bit twin: an odd pair count, pairs whose
+    ids just fit 15 bits (m + n = 32767) and pairs just past it (32768, not
+    packable), unaligned strings, shorter partners, empty sides."""
+    pairs = _packed_class_pairs(stm)
+    batch = _pack_unaligned(pairs, stm)
+    want = _batch_expected(batch)
+    got, info = _run_plan(batch, slcs.Config.make(tile_m=stm, seg=16, tile_n=4), cuda)
+    eligible = sum(1 for a, b in pairs if len(b) > 0 and len(a) + len(b) <= 32767)
+    assert info["packed_pairs"] == eligible
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("tns", [4, 8])
+def test_batch_stream_unaligned_strings(cuda, tns):
+    """32-bit stream classes on strings at odd byte offsets."""
+    pairs = _packed_class_pairs(16)
+    batch = _pack_unaligned(pairs, 5 + tns)
+    got, info = _run_plan(batch, slcs.Config.make(strand_bits=32, tile_n=tns), cuda)
+    assert info["packed_pairs"] == 0 and info["stream_pairs"] > 100
+    np.testing.assert_array_equal(got, _batch_expected(batch))
+
+
+def test_batch_packed_tiny_pairs(cuda):
+    """Couples of one-block pairs switch every step."""
+    rng = np.random.default_rng(77)
+    pairs = [(rng.integers(0, 3, int(rng.integers(1, 40)), dtype=np.uint8),
+              rng.integers(0, 3, int(rng.integers(1, 9)), dtype=np.uint8)) for _ in range(777)]
+    batch = W.pack(pairs)
+    got, info = _run_plan(batch, slcs.Config.make(tile_n=4), cuda)
+    assert info["packed_pairs"] == 777
+    np.testing.assert_array_equal(got, _batch_expected(batch))
+
+
+def _golden():
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden.json")) as f:
+        return json.load(f)
+
+
+def _sha256(x):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(x).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("name,cfg", [("pair_131072_mutated", dict()),
+                                      ("pair_1M", dict(tile_m=16, warps=8))])
+def test_pair_large_golden(cuda, name, cfg):
+    """Full-size single pairs against digests of the oracle's permutation
+    (tests/golden/make_golden.py --big wrote them)."""
+    g = _golden()[name]
+    a, b = W.pair_131072_mutated() if name == "pair_131072_mutated" else W.pair_1m()
+    h, v = slcs.comb_pair(_dev(a, cuda), _dev(b, cuda), cfg=slcs.Config.make(**cfg))
+    _, c2r = slcs.strands_to_permutation(h, v)
+    c2r = c2r.cpu().numpy()
+    slcs.device_status(0)
+    assert _sha256(c2r) == g["sha256_col_to_row"]
+    assert slcs.permutation_hash(c2r) == g["hash"]
+
+
+@pytest.mark.parametrize("cfg", [dict(), dict(strand_bits=32), dict(tile_n=8), dict(algo=1, tile_m=8)])
+def test_batch_reads_20000_golden(cuda, cfg):
+    """The 20,000-read batch against the digest of the oracle's strands."""
+    g = _golden()["reads_20000"]
+    batch = W.reads_20000()
+    assert batch.cells == g["cells"]
+    got, _ = _run_plan(batch, slcs.Config.make(**cfg), cuda)
+    assert _sha256(got) == g["sha256_strands"]
