@@ -56,6 +56,7 @@ int pick_tile_m(const slcs_config *cfg, int32_t m_typical, int64_t total_cells)
 {
     if (cfg && cfg->tile_m) return cfg->tile_m;
     (void)total_cells;
+    if (m_typical >= 262144) return 16; // >= 512 stripes of 512 rows: enough warps in flight
     if (m_typical >= 65536) return 8;
     if (m_typical >= 8192) return 4;
     if (m_typical <= 64) return 2;
@@ -63,7 +64,8 @@ int pick_tile_m(const slcs_config *cfg, int32_t m_typical, int64_t total_cells)
     return 8;
 }
 
-int pick_warps(const slcs_config *cfg) { return (cfg && cfg->warps) ? cfg->warps : 4; }
+// 16 rows per lane leave room for 8 warps per block; the smaller tiles run 4.
+int pick_warps(const slcs_config *cfg, int tm) { return (cfg && cfg->warps) ? cfg->warps : (tm == 16 ? 8 : 4); }
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -342,13 +344,13 @@ slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_
     L.single.out_off = 0;
     slcs_status s;
     if (v_out == h_out + m) {
-        s = launch_comb(L, tm, pick_warps(cfg), st, nullptr);
+        s = launch_comb(L, tm, pick_warps(cfg, tm), st, nullptr);
     } else {
         // Comb into a contiguous temporary, then copy v out.
         int32_t *tmp = nullptr;
         SLCS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&tmp), sizeof(int32_t) * (size_t(m) + n), st));
         L.out = tmp;
-        s = launch_comb(L, tm, pick_warps(cfg), st, nullptr);
+        s = launch_comb(L, tm, pick_warps(cfg, tm), st, nullptr);
         if (s == SLCS_OK) {
             SLCS_CUDA(cudaMemcpyAsync(h_out, tmp, sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, st));
             SLCS_CUDA(cudaMemcpyAsync(v_out, tmp + m, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
@@ -421,7 +423,7 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
         std::nth_element(ms.begin(), ms.begin() + ms.size() / 2, ms.end());
         med = ms[ms.size() / 2];
     }
-    P->warps = pick_warps(cfg);
+    P->warps = pick_warps(cfg, pick_tile_m(cfg, med, cells));
     P->use_graph = cfg && cfg->use_graph;
     P->wait_ns = wait_limit_ns(cfg);
     P->npairs = npairs;
@@ -468,7 +470,7 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
             P->classes.push_back({16, 32, false});
         }
         for (const auto &c : P->classes)
-            if (!stream_variant_supported(c.tm, c.seg)) {
+            if (c.packed ? !packed16_supported(c.tm, c.seg) : !stream_variant_supported(c.tm, c.seg)) {
                 delete P;
                 return fail(SLCS_ERR_UNSUPPORTED, "stream mode needs tile_m in {4,8,12,16} and seg in {8,16,32}");
             }
@@ -519,7 +521,11 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
                 if (pairs[p].m <= k.tm * k.seg && (!k.packed || int64_t(pairs[p].m) + pairs[p].n <= PACKED16_MAX_IDS))
                     break;
             }
-            cls_pairs[std::min(c, nclass - 1)].push_back(p);
+            if (c == nclass) { // cannot happen: the tallest class is a 32-bit one
+                delete P;
+                return fail(SLCS_ERR_INVALID, "internal: no stream class for a pair");
+            }
+            cls_pairs[c].push_back(p);
         }
         std::vector<std::vector<std::pair<int32_t, int32_t>>> items(nclass);
         for (int c = 0; c < nclass; ++c) {
@@ -532,16 +538,21 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
                 for (int32_t p : cp) items[c].push_back({p, -1});
             }
         }
-        auto cost = [&](const std::pair<int32_t, int32_t> &it) {
+        // Cost of an item: its column blocks plus a pair switch, in steps.
+        // (Weighting steps by the instructions of a class made the plans
+        // slower on the GPU: a warp's speed is not set by its own share of
+        // the integer pipes alone.)
+        auto cost = [&](int c, const std::pair<int32_t, int32_t> &it) {
+            const int cols = P->classes[c].packed ? 4 : P->tns;
             const int32_t n = std::max(pairs[it.first].n, it.second >= 0 ? pairs[it.second].n : 0);
-            return int64_t((n + P->tns - 1) / P->tns) + 2;
+            return int64_t((n + cols - 1) / cols) + 2;
         };
         std::vector<double> wsteps(nclass, 0.0);
         std::vector<long> wmax(nclass, 0);
         double total = 0.0;
         for (int c = 0; c < nclass; ++c) {
             int64_t w = 0;
-            for (const auto &it : items[c]) w += cost(it);
+            for (const auto &it : items[c]) w += cost(c, it);
             const int spw = 32 / P->classes[c].seg;
             wsteps[c] = double(w) / spw;
             wmax[c] = (long(items[c].size()) + spw - 1) / spw;
@@ -586,14 +597,14 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
             for (long sgi = 0; sgi < nseg; ++sgi) heap.push({0, sgi});
             std::stable_sort(items[c].begin(), items[c].end(),
                              [&](const std::pair<int32_t, int32_t> &x, const std::pair<int32_t, int32_t> &y) {
-                                 return cost(x) > cost(y);
+                                 return cost(c, x) > cost(c, y);
                              });
             for (const auto &it : items[c]) {
                 Load top = heap.top();
                 heap.pop();
                 const long warp = wbase + top.second / spw, sidx = top.second % spw;
                 slot_lists[size_t(warp) * SEG_SLOTS + size_t(sidx)].push_back(it);
-                top.first += cost(it);
+                top.first += cost(c, it);
                 heap.push(top);
             }
             wbase += wc[c];

@@ -270,7 +270,7 @@ template <int TM>
 struct NextPair {
     int pair;
     int4 d0, d1; // PairDev: a_off, b_off | out_off, m, n
-    uint32_t sym[TM / 4];
+    uint32_t sym[(TM + 3) / 4];
 };
 
 template <int TM>
@@ -284,12 +284,13 @@ __device__ __forceinline__ void fetch_next(const CombLaunch &L, int pair, int r0
     const int64_t a_off = int64_t((uint64_t(uint32_t(N.d0.y)) << 32) | uint32_t(N.d0.x));
     const int m = N.d1.z;
     const uint8_t *a = L.a_blob + a_off + r0;
-    if (r0 + TM <= m && (reinterpret_cast<uintptr_t>(a) & 3) == 0) {
+    constexpr int WORDS = (TM + 3) / 4;
+    if (r0 + 4 * WORDS <= m && (reinterpret_cast<uintptr_t>(a) & 3) == 0) {
 #pragma unroll
-        for (int q = 0; q < TM / 4; ++q) N.sym[q] = __ldg(reinterpret_cast<const uint32_t *>(a) + q);
+        for (int q = 0; q < WORDS; ++q) N.sym[q] = __ldg(reinterpret_cast<const uint32_t *>(a) + q);
     } else {
 #pragma unroll
-        for (int q = 0; q < TM / 4; ++q) {
+        for (int q = 0; q < WORDS; ++q) {
             uint32_t w = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k)
@@ -597,6 +598,8 @@ __device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int seg_i
 #define SLCS_STREAM_CLASSES(X) X(4, 8) X(4, 16) X(4, 32) X(8, 8) X(8, 16) X(8, 32) \
     X(12, 8) X(12, 16) X(12, 32) X(16, 8) X(16, 16) X(16, 32)
 // Packed classes (4 columns per step).
+// (Packed classes of 6, 10 and 14 rows per lane halve the row padding, but
+// compiled into this kernel they slowed every class down by 10-15 %.)
 #define SLCS_PACKED_CLASSES(X) X(4, 16) X(8, 16) X(12, 16) X(16, 16)
 
 template <int TNS, int WARPS>

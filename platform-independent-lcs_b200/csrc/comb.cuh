@@ -29,7 +29,7 @@ struct CombLaunch {
 // (whole warps, tile_m rows per lane), then every single-stripe pair is
 // streamed: a segment of `seg` lanes combs pair after pair without draining
 // its pipeline between them.
-constexpr int MAX_CLASSES = 10;
+constexpr int MAX_CLASSES = 12;
 constexpr int SEG_SLOTS = 4; // segment slots per warp (32 / smallest SEG)
 struct BatchLaunch {
     CombLaunch wf;           // wavefront part (tasks of pairs too tall to stream)

@@ -26,10 +26,11 @@ MODEL_PATH = os.path.join(HERE, "data", "costmodel.json")
 # The variants the autotuner times and the model ranks.  Variant 0 is what the
 # library does when nothing is configured (the fixed heuristic).
 VARIANTS: List[dict] = [
-    {"name": "stream_tn8", "cfg": {}},
-    {"name": "stream_tn4", "cfg": {"tile_n": 4}},
-    {"name": "stream_tn8_bpsm2", "cfg": {"blocks_per_sm": 2}},
-    {"name": "stream_tn4_bpsm2", "cfg": {"tile_n": 4, "blocks_per_sm": 2}},
+    {"name": "stream_auto", "cfg": {}},
+    {"name": "stream_tn8_32", "cfg": {"strand_bits": 32}},
+    {"name": "stream_tn4_32", "cfg": {"strand_bits": 32, "tile_n": 4}},
+    {"name": "stream_auto_bpsm2", "cfg": {"blocks_per_sm": 2}},
+    {"name": "stream_tn8_32_bpsm2", "cfg": {"strand_bits": 32, "blocks_per_sm": 2}},
     {"name": "wavefront_tm2", "cfg": {"algo": 1, "tile_m": 2}},
     {"name": "wavefront_tm4", "cfg": {"algo": 1, "tile_m": 4}},
     {"name": "wavefront_tm8", "cfg": {"algo": 1, "tile_m": 8}},
@@ -38,7 +39,7 @@ VARIANTS: List[dict] = [
     {"name": "wavefront_tm8_w8", "cfg": {"algo": 1, "tile_m": 8, "warps": 8}},
 ]
 HEURISTIC = 0
-PLAIN = 6  # the plain wavefront kernel with its default tile
+PLAIN = 7  # the plain wavefront kernel with its default tile
 
 
 def variant_config(i: int, use_graph: bool = True) -> Config:

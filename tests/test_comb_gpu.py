@@ -327,3 +327,19 @@ def test_batch_reads_20000_golden(cuda, cfg):
     assert batch.cells == g["cells"]
     got, _ = _run_plan(batch, slcs.Config.make(**cfg), cuda)
     assert _sha256(got) == g["sha256_strands"]
+
+
+def test_batch_default_plan_all_row_classes(cuda):
+    """Rows 1..600 through the default plan: the four packed row classes
+    (4..16 rows per lane, 16 lanes), 32-bit classes and wavefront tasks."""
+    rng = np.random.default_rng(4242)
+    pairs = []
+    for i in range(1201):
+        m = int(rng.integers(1, 601))
+        n = int(rng.integers(1, 400)) if i % 97 else 32768 - min(m, 256)  # not packable
+        sigma = int(rng.choice([2, 4, 256]))
+        pairs.append((rng.integers(0, sigma, m, dtype=np.uint8), rng.integers(0, sigma, n, dtype=np.uint8)))
+    batch = _pack_unaligned(pairs, 4242)
+    got, info = _run_plan(batch, slcs.Config.make(), cuda)
+    assert info["stream_classes"] >= 6 and info["wavefront_tasks"] > 0
+    np.testing.assert_array_equal(got, _batch_expected(batch))
