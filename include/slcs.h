@@ -183,6 +183,12 @@ SLCS_API slcs_status slcs_batch_plan_info(const slcs_batch_plan *plan, slcs_plan
 SLCS_API slcs_status slcs_strands_to_permutation(const int32_t *h, int32_t m, const int32_t *v, int32_t n,
                                         int32_t *row_to_col, int32_t *col_to_row, void *stream);
 
+/* The inverse of slcs_strands_to_permutation: strands h (m) and v (n) of the
+ * permutation P(a, b) given as row_to_col (size m+n), e.g. the product of
+ * slcs_braid_multiply that glued column strips of one pair. */
+SLCS_API slcs_status slcs_permutation_to_strands(const int32_t *row_to_col, int32_t m, int32_t n, int32_t *h,
+                                                 int32_t *v, void *stream);
+
 /* PermutationMatrix::hash (src/permutation_matrix.hpp:192-203) of a host
  * col_to_row array, with the reference's signed 64-bit wrap-around. */
 SLCS_API int64_t slcs_permutation_hash(const int32_t *col_to_row, int32_t size);

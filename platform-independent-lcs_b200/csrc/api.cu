@@ -13,6 +13,7 @@
 
 #include "braid.cuh"
 #include "comb.cuh"
+#include "strips.cuh"
 
 namespace slcs {
 
@@ -316,6 +317,7 @@ slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_
     if (m == 0 || n == 0) return write_identity(h_out, m, v_out, n, st);
     const int tm = pick_tile_m(cfg, m, int64_t(m) * n);
     if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+    if (cfg && cfg->algo == SLCS_ALGO_STRIPS) return comb_strips(a, m, b, n, h_out, v_out, cfg, tm, pick_warps(cfg, tm), st);
     const int32_t ntasks = stripes_of(m, tm);
     const size_t work_bytes = align_up(sizeof(int32_t) * (4 + size_t(ntasks)), 256);
     const size_t scr_bytes = sizeof(int32_t) * size_t(scratch_elems(m, n, tm));
@@ -828,6 +830,16 @@ slcs_status slcs_strands_to_permutation(const int32_t *h, int32_t m, const int32
     if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
     if ((m > 0 && !h) || (n > 0 && !v)) return fail(SLCS_ERR_INVALID, "null strands");
     return launch_strands_to_perm(h, m, v, n, row_to_col, col_to_row, static_cast<cudaStream_t>(stream));
+}
+
+slcs_status slcs_permutation_to_strands(const int32_t *row_to_col, int32_t m, int32_t n, int32_t *h, int32_t *v,
+                                        void *stream)
+{
+    if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
+    if (int64_t(m) + n > INT32_MAX) return fail(SLCS_ERR_RANGE, "m+n exceeds int32 strand ids");
+    if ((m + n > 0 && !row_to_col) || (m > 0 && !h) || (n > 0 && !v))
+        return fail(SLCS_ERR_INVALID, "null permutation or strands");
+    return perm_to_strands(row_to_col, m, n, h, v, static_cast<cudaStream_t>(stream));
 }
 
 // Restates PermutationMatrix::hash (src/permutation_matrix.hpp:192-203): the

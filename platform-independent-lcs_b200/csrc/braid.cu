@@ -37,6 +37,9 @@ namespace {
 constexpr int SCAN_BS = 2048;   // elements per block of the device-wide scan
 constexpr int SUB_THREADS = 512; // threads of the subtree block
 constexpr int SUB_MAX = 4096;   // largest node a block finishes in shared memory
+// Shared memory of a subtree block for nodes of up to maxn entries: eight
+// int16 arrays and two byte arrays.
+constexpr size_t subtree_smem(int maxn) { return size_t(maxn) * 2 * 8 + size_t(maxn) * 2; }
 
 __host__ __device__ __forceinline__ void node_of(int i, int level, int k, int &o, int &s)
 {
@@ -251,7 +254,7 @@ struct NodeView {
 // dominance-count updates (dom_sum_count, 39-119).  Fresh points are written
 // straight into `res` (row -> col) on top of the glued union.
 template <typename V, typename ResT>
-__device__ void ant_walk_seq(const V &N, ResT *res)
+__device__ __forceinline__ void ant_walk_seq(const V N, ResT *__restrict__ res)
 {
     const int n = N.n;
     int cur_row = n, cur_col = -1;
@@ -313,6 +316,7 @@ __device__ void ant_walk_seq(const V &N, ResT *res)
 // ---------------------------------------------------------------------------
 // block-wide scans for the subtree kernel
 // ---------------------------------------------------------------------------
+template <int THREADS>
 __device__ __forceinline__ void block_scan2(int &a, int &b, int *wa, int *wb)
 {
     // inclusive scan of (a, b) across the block; returns exclusive values
@@ -331,8 +335,8 @@ __device__ __forceinline__ void block_scan2(int &a, int &b, int *wa, int *wb)
     }
     __syncthreads();
     if (threadIdx.x < 32) {
-        int sa = threadIdx.x < SUB_THREADS / 32 ? wa[threadIdx.x] : 0;
-        int sb = threadIdx.x < SUB_THREADS / 32 ? wb[threadIdx.x] : 0;
+        int sa = threadIdx.x < THREADS / 32 ? wa[threadIdx.x] : 0;
+        int sb = threadIdx.x < THREADS / 32 ? wb[threadIdx.x] : 0;
         for (int off = 1; off < 32; off <<= 1) {
             int ya = __shfl_up_sync(FULL_MASK, sa, off), yb = __shfl_up_sync(FULL_MASK, sb, off);
             if (threadIdx.x >= off) {
@@ -340,7 +344,7 @@ __device__ __forceinline__ void block_scan2(int &a, int &b, int *wa, int *wb)
                 sb += yb;
             }
         }
-        if (threadIdx.x < SUB_THREADS / 32) {
+        if (threadIdx.x < THREADS / 32) {
             wa[threadIdx.x] = sa;
             wb[threadIdx.x] = sb;
         }
@@ -360,9 +364,12 @@ struct SubArgs {
     const int32_t *bad;
 };
 
-// One block finishes the subtree of one node of level lc (size <= SUB_MAX):
-// every deeper level, down then up, in shared memory.
-__global__ void __launch_bounds__(SUB_THREADS) subtree_kernel(SubArgs A)
+// One block finishes the subtree of one node of level lc (size <= MAXN):
+// every deeper level, down then up, in shared memory.  Smaller variants
+// (fewer threads, less shared memory) keep more blocks resident per SM when
+// the cutoff is small.
+template <int MAXN, int THREADS>
+__global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
 {
     if (*A.bad) return;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -378,18 +385,18 @@ __global__ void __launch_bounds__(SUB_THREADS) subtree_kernel(SubArgs A)
         }
     }
     int16_t *Pa = reinterpret_cast<int16_t *>(smem);
-    int16_t *Qa = Pa + SUB_MAX;
-    int16_t *Pb = Qa + SUB_MAX;
-    int16_t *Qb = Pb + SUB_MAX;
-    int16_t *C = Qb + SUB_MAX;
-    int16_t *R = C + SUB_MAX;
-    int16_t *ResA = R + SUB_MAX;
-    int16_t *ResB = ResA + SUB_MAX;
-    uint8_t *H = reinterpret_cast<uint8_t *>(ResB + SUB_MAX);
-    uint8_t *HC = H + SUB_MAX;
+    int16_t *Qa = Pa + MAXN;
+    int16_t *Pb = Qa + MAXN;
+    int16_t *Qb = Pb + MAXN;
+    int16_t *C = Qb + MAXN;
+    int16_t *R = C + MAXN;
+    int16_t *ResA = R + MAXN;
+    int16_t *ResB = ResA + MAXN;
+    uint8_t *H = reinterpret_cast<uint8_t *>(ResB + MAXN);
+    uint8_t *HC = H + MAXN;
     __shared__ int wa[32], wb[32];
 
-    for (int i = threadIdx.x; i < S; i += SUB_THREADS) {
+    for (int i = threadIdx.x; i < S; i += THREADS) {
         Pa[i] = int16_t(A.P[o + i]);
         Qa[i] = int16_t(A.Q[o + i]);
     }
@@ -399,7 +406,7 @@ __global__ void __launch_bounds__(SUB_THREADS) subtree_kernel(SubArgs A)
     int depth = 0;
     for (int s = S; s > 1; s = s - (s >> 1)) ++depth;
 
-    constexpr int PER = SUB_MAX / SUB_THREADS;
+    constexpr int PER = MAXN / THREADS;
     for (int d = 0; d < depth; ++d) {
         int fp[PER], fq[PER], cp = 0, cq = 0;
         const int i0 = threadIdx.x * PER;
@@ -418,7 +425,7 @@ __global__ void __launch_bounds__(SUB_THREADS) subtree_kernel(SubArgs A)
             cq += fq[j];
         }
         int ep = cp, eq = cq;
-        block_scan2(ep, eq, wa, wb);
+        block_scan2<THREADS>(ep, eq, wa, wb);
         // exclusive scan values stored in ResA/ResB (free during the descent)
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
@@ -433,7 +440,7 @@ __global__ void __launch_bounds__(SUB_THREADS) subtree_kernel(SubArgs A)
         __syncthreads();
         int32_t *pmap = A.maps + size_t(2) * A.k * (A.lc + d + 1);
         int32_t *qmap = pmap + A.k;
-        for (int i = threadIdx.x; i < S; i += SUB_THREADS) {
+        for (int i = threadIdx.x; i < S; i += THREADS) {
             int so, ss;
             node_of(i, d, S, so, ss);
             const int h = ss >> 1, local = i - so;
@@ -463,14 +470,14 @@ __global__ void __launch_bounds__(SUB_THREADS) subtree_kernel(SubArgs A)
     }
 
     // leaves: every node of the deepest level has size 1 (product = identity)
-    for (int i = threadIdx.x; i < S; i += SUB_THREADS) ResB[i] = 0;
+    for (int i = threadIdx.x; i < S; i += THREADS) ResB[i] = 0;
     __syncthreads();
 
     for (int d = depth - 1; d >= 0; --d) {
         const int32_t *pmap = A.maps + size_t(2) * A.k * (A.lc + d + 1);
         const int32_t *qmap = pmap + A.k;
         // glue: children at level d+1 into parents at level d
-        for (int i = threadIdx.x; i < S; i += SUB_THREADS) {
+        for (int i = threadIdx.x; i < S; i += THREADS) {
             int po, ps, co, cs;
             node_of(i, d, S, po, ps);
             if (ps <= 1) {
@@ -487,7 +494,7 @@ __global__ void __launch_bounds__(SUB_THREADS) subtree_kernel(SubArgs A)
             HC[po + pcol] = hi;
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < S; i += SUB_THREADS) {
+        for (int i = threadIdx.x; i < S; i += THREADS) {
             int po, ps;
             node_of(i, d, S, po, ps);
             if (ps > 1) ResA[i] = C[i];
@@ -495,7 +502,7 @@ __global__ void __launch_bounds__(SUB_THREADS) subtree_kernel(SubArgs A)
         __syncthreads();
         // walks: one thread per node of level d
         const int nodes = 1 << d;
-        for (int nd = threadIdx.x; nd < nodes; nd += SUB_THREADS) {
+        for (int nd = threadIdx.x; nd < nodes; nd += THREADS) {
             int po = 0, ps = S;
             for (int e = 0; e < d; ++e) {
                 const int h = ps >> 1;
@@ -515,7 +522,7 @@ __global__ void __launch_bounds__(SUB_THREADS) subtree_kernel(SubArgs A)
         ResA = ResB;
         ResB = t;
     }
-    for (int i = threadIdx.x; i < S; i += SUB_THREADS) A.res[o + i] = S > 1 ? ResB[i] : 0;
+    for (int i = threadIdx.x; i < S; i += THREADS) A.res[o + i] = S > 1 ? ResB[i] : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -553,28 +560,6 @@ __global__ void __launch_bounds__(256) union_kernel(const int32_t *C, int32_t *r
 {
     if (*bad) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) res[i] = C[i];
-}
-
-// One thread per node of the level: the sequential walk in global memory.
-__global__ void __launch_bounds__(128) walk_seq_kernel(GlueArgs A)
-{
-    if (*A.bad) return;
-    const int nodes = 1 << A.level;
-    const int nd = blockIdx.x * blockDim.x + threadIdx.x;
-    if (nd >= nodes) return;
-    int o = 0, s = A.k;
-    for (int e = 0; e < A.level; ++e) {
-        const int h = s >> 1;
-        if ((nd >> (A.level - 1 - e)) & 1) {
-            o += h;
-            s -= h;
-        } else {
-            s = h;
-        }
-    }
-    if (s <= 1) return;
-    NodeView<int32_t, uint8_t> N{A.C + o, A.H + o, A.R + o, A.HC + o, s};
-    ant_walk_seq(N, A.res + o);
 }
 
 // ---------------------------------------------------------------------------
@@ -1172,17 +1157,26 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     }
     // Nodes of level lc: one block each, down to the leaves and back.
     {
-        const size_t smem = size_t(SUB_MAX) * 2 * 8 + size_t(SUB_MAX) * 2;
-        static bool attr[64] = {};
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev < 0 || dev >= 64) dev = 0;
-        if (!attr[dev]) {
-            SLCS_CUDA(cudaFuncSetAttribute(subtree_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-            attr[dev] = true;
-        }
+        int smax = k; // largest node of level lc (floor/ceil halving)
+        for (int l = 0; l < lc; ++l) smax = smax - (smax >> 1);
         SubArgs S{Pcur, Qcur, res + kk * size_t(lc), maps, k, lc, bad};
-        subtree_kernel<<<1 << lc, SUB_THREADS, smem, st>>>(S);
+        if (smax <= 256) {
+            subtree_kernel<256, 128><<<1 << lc, 128, subtree_smem(256), st>>>(S);
+        } else if (smax <= 1024) {
+            subtree_kernel<1024, 256><<<1 << lc, 256, subtree_smem(1024), st>>>(S);
+        } else {
+            static bool attr[64] = {};
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (dev < 0 || dev >= 64) dev = 0;
+            if (!attr[dev]) {
+                SLCS_CUDA(cudaFuncSetAttribute(subtree_kernel<SUB_MAX, SUB_THREADS>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, int(subtree_smem(SUB_MAX))));
+                attr[dev] = true;
+            }
+            subtree_kernel<SUB_MAX, SUB_THREADS><<<1 << lc, SUB_THREADS, subtree_smem(SUB_MAX), st>>>(S);
+        }
+        SLCS_CUDA(cudaGetLastError());
     }
     // Levels above: glue, union, walk.
     for (int l = lc - 1; l >= 0; --l) {

@@ -91,6 +91,7 @@ def lib():
         L.slcs_batch_plan_launches.restype = _i32
         L.slcs_batch_plan_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
         L.slcs_strands_to_permutation.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, _vp]
+        L.slcs_permutation_to_strands.argtypes = [_vp, _i32, _i32, _vp, _vp, _vp]
         L.slcs_permutation_hash.argtypes = [_vp, _i32]
         L.slcs_permutation_hash.restype = _i64
         L.slcs_probe_int_rates.argtypes = [_i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _vp]
@@ -234,6 +235,17 @@ def strands_to_permutation(h, v, stream=None):
     c2r = torch.empty(m + n, dtype=torch.int32, device=h.device)
     check(lib().slcs_strands_to_permutation(_dptr(h), m, _dptr(v), n, _dptr(r2c), _dptr(c2r), _stream(stream)))
     return r2c, c2r
+
+
+def permutation_to_strands(r2c, m: int, stream=None):
+    """(h, v) strands of P(a, b) from its row -> col array (size m + n)."""
+    import torch
+    size = int(r2c.numel())
+    n = size - int(m)
+    out = torch.empty(size, dtype=torch.int32, device=r2c.device)
+    check(lib().slcs_permutation_to_strands(_dptr(r2c), int(m), n, _dptr(out), _dptr(out) + 4 * int(m) if n else 0,
+                                            _stream(stream)))
+    return out[:m], out[m:]
 
 
 def permutation_hash(col_to_row: np.ndarray) -> int:

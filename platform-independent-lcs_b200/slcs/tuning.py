@@ -93,4 +93,63 @@ def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev):
                         "roofline_frac": g / roof_gcups, "hash": hv,
                         "bitexact_vs_reference": (hv == gold) if gold is not None else None,
                         "variant": {"tile_m": 16, "warps": 8}}
+    res.update(strips_and_braid(ad, bd, o, gold, dev))
     return res
+
+
+def _measured_hbm_gbs():
+    try:
+        with open(os.path.join(HERE, "..", "..", "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json (copy, read+write bytes)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def strips_and_braid(ad, bd, o, gold_hash, dev):
+    """The 2^20 x 2^20 pair as 8 column strips glued by braid products, over
+    the cutoff sweep {64, 256, 1024, 4096}; and one braid product alone (the
+    top merge of the two halves of b, overlap k = 2^20) against HBM."""
+    import torch
+    from . import braid_multiply, comb_pair
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m, n = int(ad.numel()), int(bd.numel())
+    cells = m * n
+
+    def timed(fn, reps=2):
+        fn()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(reps):
+            e0.record(st)
+            fn()
+            e1.record(st)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+    sweep = {}
+    for cutoff in (64, 256, 1024, 4096):
+        cfg = Config.make(algo=2, strips=8, braid_cutoff=cutoff)
+        ms = timed(lambda: comb_pair(ad, bd, cfg=cfg, out=o))
+        _, c2r = strands_to_permutation(o[:m], o[m:])
+        hv = permutation_hash(c2r.cpu().numpy())
+        sweep[str(cutoff)] = {"ms": ms, "gcups": cells / (ms * 1e-3) / 1e9,
+                              "bitexact_vs_reference": (hv == gold_hash) if gold_hash is not None else None}
+    half = n // 2
+    hp, vp = comb_pair(ad, bd[:half])
+    hq, vq = comb_pair(ad, bd[half:])
+    P = strands_to_permutation(hp, vp)[0]
+    Q = strands_to_permutation(hq, vq)[0]
+    peak, peak_src = _measured_hbm_gbs()
+    braid = {}
+    for cutoff in (64, 256, 1024, 4096):
+        cfg = Config.make(braid_cutoff=cutoff)
+        ms = timed(lambda: braid_multiply(P, Q, m, False, cfg=cfg), reps=3)
+        p, q = int(P.numel()), int(Q.numel())
+        algo_bytes = 4 * (p + q) + 4 * (p + q - m)
+        gbs = algo_bytes / (ms * 1e-3) / 1e9
+        braid[str(cutoff)] = {"ms": ms, "algorithmic_bytes": algo_bytes, "achieved_gbs": gbs, "frac": gbs / peak}
+    return {"long_pair_strips": {"workload": "pair_1M as 8 column strips + braid merge tree", "cutoff_sweep": sweep},
+            "braid_top_merge": {"workload": "staggered_multiply<false>(P(a,b[:n/2]), P(a,b[n/2:]), k=2^20)",
+                                "bound": "hbm", "peak_gbs": peak, "peak_source": peak_src, "by_cutoff": braid}}

@@ -1,0 +1,116 @@
+"""The multi-GPU split on CPU processes (gloo, world sizes 2 and 3): strip
+widths, the merge schedule, LPT sharding, and the send/recv merge tree of one
+long pair, with the compute steps done by the CPU oracle so that the exchange
+logic is checked without a GPU."""
+import os
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle as O
+from slcs import distributed as D
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def test_strip_widths():
+    for n in (0, 1, 15, 16, 100, 4096, 131072, 1000003):
+        for s in (1, 2, 3, 8):
+            w = D.strip_widths(n, s)
+            assert len(w) == s and sum(w) == n and min(w) >= 0
+            assert all(w[i] % 16 == 0 or sum(w[i + 1:]) == 0 for i in range(s - 1))
+
+
+def test_merge_rounds_cover_every_rank_once():
+    for world in range(1, 9):
+        alive = set(range(world))
+        for rnd in D.merge_rounds(world):
+            for dst, src in rnd:
+                assert dst in alive and src in alive and dst < src
+                alive.discard(src)
+        assert alive == {0}
+
+
+def test_shard_pairs_lpt():
+    rng = np.random.default_rng(3)
+    cells = rng.integers(1, 10**6, 5000)
+    for world in (1, 2, 3, 8):
+        shards = D.shard_pairs(cells, world)
+        assert sorted(np.concatenate(shards).tolist()) == list(range(len(cells)))
+        loads = [int(cells[s].sum()) for s in shards]
+        assert max(loads) - min(loads) <= int(cells.max())
+
+
+class OracleKernels:
+    """CPU stand-ins for the compute steps (torch CPU tensors)."""
+
+    def comb(self, a, b):
+        import torch
+        h, v = O.comb(a.numpy(), b.numpy())
+        return torch.from_numpy(h), torch.from_numpy(v)
+
+    def to_perm(self, h, v):
+        import torch
+        return torch.from_numpy(O.from_strands(h.numpy(), v.numpy())[0])
+
+    def braid(self, p, q, k):
+        import torch
+        return torch.from_numpy(O.staggered_multiply(p.numpy(), q.numpy(), k, False)[0])
+
+    def to_strands(self, r2c, m):
+        import torch
+        r = r2c.numpy()
+        n = len(r) - m
+        h = np.empty(m, np.int32)
+        v = np.empty(n, np.int32)
+        rows = np.arange(len(r), dtype=np.int32)
+        v[r[r < n]] = rows[r < n]
+        h[r[r >= n] - n] = rows[r >= n]
+        return torch.from_numpy(h), torch.from_numpy(v)
+
+    def empty(self, size, like):
+        import torch
+        return torch.empty(int(size), dtype=torch.int32)
+
+
+def _worker(rank, world, port, m, n, seed, out_path):
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(seed)
+        a = torch.from_numpy(rng.integers(0, 4, m, dtype=np.uint8))
+        b = torch.from_numpy(rng.integers(0, 4, n, dtype=np.uint8))
+        res = D.comb_pair_distributed(a, b, kernels=OracleKernels())
+        if rank == 0:
+            np.savez(out_path, h=res[0].numpy(), v=res[1].numpy())
+        else:
+            assert res is None
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,m,n", [(2, 300, 1000), (3, 257, 777), (2, 100, 20)])
+def test_comb_pair_distributed_gloo(world, m, n):
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    seed = 17 + world + m
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "res.npz")
+        mp.start_processes(_worker, args=(world, port, m, n, seed, out), nprocs=world, join=True,
+                           start_method="spawn")
+        got = np.load(out)
+        rng = np.random.default_rng(seed)
+        a = rng.integers(0, 4, m, dtype=np.uint8)
+        b = rng.integers(0, 4, n, dtype=np.uint8)
+        eh, ev = O.comb(a, b)
+        np.testing.assert_array_equal(got["h"], eh)
+        np.testing.assert_array_equal(got["v"], ev)
