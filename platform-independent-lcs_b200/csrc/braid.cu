@@ -27,6 +27,7 @@
 //     below-right) is non-negative, so a segment can start anywhere once r* is
 //     known there (see walk_segments).
 #include <climits>
+#include <cmath>
 #include <vector>
 
 #include "braid.cuh"
@@ -755,8 +756,13 @@ __device__ int delta_at(const SegArgs &A, const int32_t *T, int o, int r, int c,
     return T[i0 * A.stride + j0] + warp_sum(acc);
 }
 
+// Rows and columns a walk segment can touch, staged per warp in shared
+// memory (packed: position | hi flag in bit 31) before lane 0 walks.
+constexpr int WALK_WIN = 1032;
+
 __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes)
 {
+    __shared__ int32_t win_r[4][WALK_WIN], win_c[4][WALK_WIN];
     if (*A.bad) return;
     const int lane = threadIdx.x & 31;
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -820,20 +826,48 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
         if (dr < 0 || dc > s) return;
         delta = delta_at(A, T, o, dr, dc, lane);
     }
-    if (lane != 0) return;
     (void)G;
+    // The segment walks at most B + 1 steps, each one row up or one column
+    // right: rows [dr - B - 2, dr] and columns [dc - 1, dc + B + 1] cover it.
+    // The warp stages them (coalesced) so that lane 0 walks in shared memory.
+    const int wi = threadIdx.x >> 5;
+    const int rb = max(0, dr - B - 2), nr = min(max(dr - rb + 1, 0), WALK_WIN);
+    const int cb = max(0, dc - 1), nc = min(max(min(s, dc + B + 2) - cb, 0), WALK_WIN);
+    for (int t = lane; t < nr; t += 32) win_r[wi][t] = A.C[o + rb + t] | (A.H[o + rb + t] ? INT_MIN : 0);
+    for (int t = lane; t < nc; t += 32) win_c[wi][t] = A.R[o + cb + t] | (A.HC[o + cb + t] ? INT_MIN : 0);
+    __syncwarp();
+    if (lane != 0) return;
+    // Outside the window (B > WALK_WIN - 8 only) the walk reads global memory.
+    auto rinc = [&](int r, int c) {
+        const unsigned t = unsigned(r - rb);
+        if (t < unsigned(nr)) {
+            const int w = win_r[wi][t];
+            const int cc = w & INT_MAX;
+            return w < 0 ? int(cc < c) : int(cc >= c);
+        }
+        return rowinc(A, o, r, c);
+    };
+    auto cinc = [&](int c, int r) {
+        const unsigned t = unsigned(c - cb);
+        if (t < unsigned(nc)) {
+            const int w = win_c[wi][t];
+            const int rr = w & INT_MAX;
+            return w < 0 ? int(rr < r) : int(rr >= r);
+        }
+        return colinc(A, o, c, r);
+    };
     const int last = E + B;
     while (dr >= 0 && dc <= s && dc - dr <= last) {
         if (dc > 0) {
-            const int dl = delta - colinc(A, o, dc - 1, dr);
-            const int dd = delta + rowinc(A, o, dr, dc);
+            const int dl = delta - cinc(dc - 1, dr);
+            const int dd = delta + rinc(dr, dc);
             if (dl < 0 && dd > 0) A.res[o + dr] = dc - 1;
         }
         if (delta < 0) {
-            if (dc + 1 <= s) delta += colinc(A, o, dc, dr);
+            if (dc + 1 <= s) delta += cinc(dc, dr);
             ++dc;
         } else if (delta == 0) {
-            if (dr - 1 >= 0) delta -= rowinc(A, o, dr - 1, dc);
+            if (dr - 1 >= 0) delta -= rinc(dr - 1, dc);
             --dr;
         } else {
             break;
@@ -1028,11 +1062,16 @@ __global__ void report_bad_kernel(const int32_t *bad, uint32_t *status)
 
 // Grid spacing and table stride of the concurrent walk at `level` (nodes of at
 // most smax entries).
+// Grid spacing of a level's delta tables: at most WALK_GMAX lines per node and
+// about 2^21 table entries per level over all its nodes (the tables are
+// rebuilt every level, and a segment walk of B steps is cheap in shared memory).
 static void walk_grid(int k, int level, int &B, int &stride)
 {
     int smax = k;
     for (int d = 0; d < level; ++d) smax = smax - (smax >> 1);
-    B = std::max(WALK_BMIN, (smax + WALK_GMAX - 1) / WALK_GMAX);
+    const double per_node = double(1 << 21) / double(1u << std::min(level, 30));
+    const int gmax = std::max(1, std::min(WALK_GMAX, int(std::sqrt(per_node)) - 1));
+    B = std::max(WALK_BMIN, (smax + gmax - 1) / gmax);
     stride = smax / B + 1;
 }
 
