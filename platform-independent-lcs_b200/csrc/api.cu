@@ -40,6 +40,16 @@ DeviceState &dev_state()
         s.init = true;
         cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, d);
         if (s.sms <= 0) s.sms = 148;
+        // Workspaces come from cudaMallocAsync on every call; by default the
+        // process's pool returns freed memory to the driver at each
+        // synchronisation, and mapping it again cost milliseconds per call.
+        // Keep it in the pool (a setting of this process only).
+        cudaMemPool_t pool = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&pool, d) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
         void *p = nullptr;
         if (cudaHostAlloc(&p, 64, cudaHostAllocMapped) == cudaSuccess) {
             s.host_status = static_cast<uint32_t *>(p);
@@ -317,6 +327,7 @@ slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_
     if (m == 0 || n == 0) return write_identity(h_out, m, v_out, n, st);
     const int tm = pick_tile_m(cfg, m, int64_t(m) * n);
     if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+    (void)sm_count(); // per-device set-up (memory pool) before the first allocation
     if (cfg && cfg->algo == SLCS_ALGO_STRIPS) return comb_strips(a, m, b, n, h_out, v_out, cfg, tm, pick_warps(cfg, tm), st);
     const int32_t ntasks = stripes_of(m, tm);
     const size_t work_bytes = align_up(sizeof(int32_t) * (4 + size_t(ntasks)), 256);
@@ -866,6 +877,7 @@ slcs_status slcs_braid_multiply(const int32_t *p_r2c, int32_t p_size, const int3
     if (p_size + q_size == 0) return SLCS_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int cutoff = (cfg && cfg->braid_cutoff > 0) ? cfg->braid_cutoff : 1024;
+    (void)sm_count(); // per-device set-up (memory pool) before the first allocation
     size_t bytes = 0;
     braid_workspace_bytes(p_size, q_size, k, cutoff, &bytes);
     void *ws = nullptr;

@@ -38,9 +38,9 @@ namespace {
 constexpr int SCAN_BS = 2048;   // elements per block of the device-wide scan
 constexpr int SUB_THREADS = 512; // threads of the subtree block
 constexpr int SUB_MAX = 4096;   // largest node a block finishes in shared memory
-// Shared memory of a subtree block for nodes of up to maxn entries: eight
-// int16 arrays and two byte arrays.
-constexpr size_t subtree_smem(int maxn) { return size_t(maxn) * 2 * 8 + size_t(maxn) * 2; }
+// Shared memory of a subtree block for nodes of up to maxn entries: two int32
+// word arrays and six int16 arrays.
+constexpr size_t subtree_smem(int maxn) { return size_t(maxn) * 4 * 2 + size_t(maxn) * 2 * 6; }
 
 __host__ __device__ __forceinline__ void node_of(int i, int level, int k, int &o, int &s)
 {
@@ -236,81 +236,87 @@ __global__ void __launch_bounds__(256) part_scatter_kernel(LevelArgs A)
 // ---------------------------------------------------------------------------
 // the ant walk (ant_passage, src/braid_multiplication.hpp:123-189)
 // ---------------------------------------------------------------------------
-// A node's glued state: C[r] = column of row r's point, H[r] = 1 if that point
-// belongs to the hi half; R[c] = row of column c's point, HC[c] likewise.
-template <typename IdxT, typename FlagT>
-struct NodeView {
-    const IdxT *C;
-    const FlagT *H;
-    const IdxT *R;
-    const FlagT *HC;
-    int n;
-    __device__ __forceinline__ int r2c_hi(int r) const { return H[r] ? int(C[r]) : -1; }
-    __device__ __forceinline__ int r2c_lo(int r) const { return H[r] ? -1 : int(C[r]); }
-    __device__ __forceinline__ int c2r_hi(int c) const { return HC[c] ? int(R[c]) : -1; }
-    __device__ __forceinline__ int c2r_lo(int c) const { return HC[c] ? -1 : int(R[c]); }
-};
-
-// Sequential walk, statement for statement the reference's loop and its
-// dominance-count updates (dom_sum_count, 39-119).  Fresh points are written
-// straight into `res` (row -> col) on top of the glued union.
-template <typename V, typename ResT>
-__device__ __forceinline__ void ant_walk_seq(const V N, ResT *__restrict__ res)
+// A node's glued state as packed words: the word of row r holds the column of
+// its point, the word of column c the row of its point, each with bit 31 set
+// when the point comes from the hi half.
+//
+// The reference keeps two dominance counts (dom_sum_count, 39-119) and moves
+// right while hi-above-left minus lo-below-right is negative, up while it is
+// zero.  Only that difference, delta(r, c) = #{hi: row < r, col < c} -
+// #{lo: row >= r, col >= c}, decides anything, and one step changes it by the
+// contribution of a single row or column:
+__device__ __forceinline__ int word_inc(int w, int lim)
 {
-    const int n = N.n;
-    int cur_row = n, cur_col = -1;
-    int rhi = 0, rlo = 0;
-    bool went_right = false;
-    for (;;) {
-        if (cur_row == 0 || cur_col == n) break;
-        const int dr = cur_row - 1, dc = cur_col + 1;
-        if (went_right) {
-            const int col = dc - 1; // right_move(dr, dc - 1)
-            if (col >= n) {
-                rhi = 0;
-                rlo = 0;
-            } else {
-                const int rh = N.c2r_hi(col), rl = N.c2r_lo(col);
-                if (rh != -1 && rh < dr) rhi++;
-                if (rl >= dr && rl != -1) rlo--;
-            }
+    const int p = w & INT_MAX;
+    return w < 0 ? int(p < lim) : int(p >= lim);
+}
+
+// Walks from the point (dr, dc) with delta = delta(dr, dc) while dr >= 0,
+// dc <= s and the diagonal dc - dr stays <= last; put(r, c) records a fresh
+// point (the reference's test at 171-181: delta left of the point negative,
+// delta below it positive).  rw(r) / cw(c) read row / column words.
+//
+// This general form serves starts with any delta.  On the walk itself delta
+// only takes the values -1 and 0: a right move (delta < 0) adds 0 or 1, an
+// up move (delta == 0) subtracts 0 or 1.  ant_walk below uses that.
+template <typename RowW, typename ColW, typename Put>
+__device__ __forceinline__ void ant_walk_general(int dr, int dc, int delta, int s, int last, RowW rw, ColW cw, Put put)
+{
+    while (dr >= 0 && dc <= s && dc - dr <= last) {
+        if (dc > 0 && delta - word_inc(cw(dc - 1), dr) < 0 && delta + word_inc(rw(dr), dc) > 0) put(dr, dc - 1);
+        if (delta < 0) {
+            if (dc + 1 <= s) delta += word_inc(cw(dc), dr);
+            ++dc;
+        } else if (delta == 0) {
+            if (dr - 1 >= 0) delta -= word_inc(rw(dr - 1), dc);
+            --dr;
         } else {
-            const int row = dr + 1; // up_move(dr + 1, dc)
-            if (row != 0) {
-                const int ch = N.r2c_hi(row - 1), cl = N.r2c_lo(row - 1);
-                if (ch != -1 && ch < dc) rhi--;
-                if (cl >= dc && cl != -1) rlo++;
-            }
+            break;
         }
-        const int d = rhi - rlo;
-        if (d < 0) {
-            went_right = true;
-            cur_col++;
-        } else if (d == 0) {
-            went_right = false;
-            cur_row--;
-        } else {
-            break; // never taken: the difference is never positive on the walk
-        }
-        if (dc > 0) {
-            // left_move(dr, dc) and down_move(dr, dc) of both counts
-            int lh = rhi, ll = rlo;
-            {
-                const int rh = N.c2r_hi(dc - 1), rl = N.c2r_lo(dc - 1);
-                if (rh != -1 && rh < dr) lh--;
-                if (rl >= dr && rl != -1) ll++;
-            }
-            int dh = rhi, dl = rlo;
-            if (dr >= n) {
-                dh = 0;
-                dl = 0;
-            } else {
-                const int ch = N.r2c_hi(dr), cl = N.r2c_lo(dr);
-                if (ch != -1 && ch < dc) dh++;
-                if (cl >= dc && cl != -1) dl--;
-            }
-            if (lh - ll < 0 && dh - dl > 0) res[dr] = ResT(dc - 1);
-        }
+    }
+}
+
+// The walk as a two-state machine (up: delta == 0, right: delta == -1).  A
+// step needs the words of rows dr, dr-1 and columns dc-1, dc, which it keeps
+// in registers; it loads the two words either move could need next before
+// deciding, and moves by selects.  The trip count only bounds the walk (each
+// step moves dc - dr up by one, and the walk leaves the box after at most
+// dr + s - dc + 1 steps), so the loop carries no data-dependent branch.
+// (A variant that also precomputed the four flip values of the step after
+// next ran slower: a lone walking warp is bound by the instructions it
+// issues per step as much as by their dependency chain.)
+template <typename RowW, typename ColW, typename Put>
+__device__ __forceinline__ void ant_walk(int dr, int dc, int delta, int s, int last, RowW rw, ColW cw, Put put)
+{
+    if (delta != 0 && delta != -1) {
+        ant_walk_general(dr, dc, delta, s, last, rw, cw, put);
+        return;
+    }
+    bool up = delta == 0;
+    bool alive = dr >= 0 && dc <= s && dc - dr <= last;
+    if (!alive) return;
+    int r0 = rw(dr);                                // row dr
+    int r1 = dr >= 1 ? rw(dr - 1) : 0;              // row dr - 1
+    int cm = dc >= 1 ? cw(dc - 1) : 0;              // column dc - 1
+    int c0 = dc < s ? cw(dc) : 0;                   // column dc
+    const int trips = int(min(int64_t(last) - (dc - dr), int64_t(dr) + s - dc)) + 1;
+#pragma unroll 4
+    for (int t = 0; t < trips; ++t) {
+        const int r2 = dr >= 2 ? rw(dr - 2) : 0;
+        const int c1 = dc + 1 < s ? cw(dc + 1) : 0;
+        if (alive && up && dc > 0 && word_inc(cm, dr) && word_inc(r0, dc)) put(dr, dc - 1);
+        const int inc_right = (dc + 1 <= s) ? word_inc(c0, dr) : 0;
+        const int inc_up = dr >= 1 ? word_inc(r1, dc) : 0;
+        const bool mv_up = alive && up, mv_right = alive && !up;
+        const bool flip = up ? inc_up : inc_right;
+        dc += mv_right;
+        dr -= mv_up;
+        cm = mv_right ? c0 : cm;
+        c0 = mv_right ? c1 : c0;
+        r0 = mv_up ? r1 : r0;
+        r1 = mv_up ? r2 : r1;
+        up = alive ? (up != flip) : up;
+        alive = alive && dr >= 0 && dc <= s && dc - dr <= last;
     }
 }
 
@@ -385,16 +391,14 @@ __global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
             S = h;
         }
     }
-    int16_t *Pa = reinterpret_cast<int16_t *>(smem);
+    int32_t *CW = reinterpret_cast<int32_t *>(smem); // row words of the node being walked
+    int32_t *RW = CW + MAXN;                         // column words
+    int16_t *Pa = reinterpret_cast<int16_t *>(RW + MAXN);
     int16_t *Qa = Pa + MAXN;
     int16_t *Pb = Qa + MAXN;
     int16_t *Qb = Pb + MAXN;
-    int16_t *C = Qb + MAXN;
-    int16_t *R = C + MAXN;
-    int16_t *ResA = R + MAXN;
+    int16_t *ResA = Qb + MAXN;
     int16_t *ResB = ResA + MAXN;
-    uint8_t *H = reinterpret_cast<uint8_t *>(ResB + MAXN);
-    uint8_t *HC = H + MAXN;
     __shared__ int wa[32], wb[32];
 
     for (int i = threadIdx.x; i < S; i += THREADS) {
@@ -488,17 +492,15 @@ __global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
             node_of(i, d + 1, S, co, cs);
             const int prow = pmap[o + i];
             const int pcol = qmap[o + co + ResB[i]];
-            const uint8_t hi = co != po;
-            C[po + prow] = int16_t(pcol);
-            H[po + prow] = hi;
-            R[po + pcol] = int16_t(prow);
-            HC[po + pcol] = hi;
+            const int hi = co != po ? INT_MIN : 0;
+            CW[po + prow] = pcol | hi;
+            RW[po + pcol] = prow | hi;
         }
         __syncthreads();
         for (int i = threadIdx.x; i < S; i += THREADS) {
             int po, ps;
             node_of(i, d, S, po, ps);
-            if (ps > 1) ResA[i] = C[i];
+            if (ps > 1) ResA[i] = int16_t(CW[i] & INT_MAX);
         }
         __syncthreads();
         // walks: one thread per node of level d
@@ -515,8 +517,10 @@ __global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
                 }
             }
             if (ps <= 1) continue;
-            NodeView<int16_t, uint8_t> N{C + po, H + po, R + po, HC + po, ps};
-            ant_walk_seq(N, ResA + po);
+            const int32_t *cw_ = CW + po, *rw_ = RW + po;
+            int16_t *res_ = ResA + po;
+            ant_walk(ps - 1, 0, cw_[ps - 1] < 0 ? 0 : -1, ps, INT_MAX, [&](int r) { return cw_[r]; },
+                     [&](int c) { return rw_[c]; }, [&](int r, int c) { res_[r] = int16_t(c); });
         }
         __syncthreads();
         int16_t *t = ResA;
@@ -758,11 +762,15 @@ __device__ int delta_at(const SegArgs &A, const int32_t *T, int o, int r, int c,
 
 // Rows and columns a walk segment can touch, staged per warp in shared
 // memory (packed: position | hi flag in bit 31) before lane 0 walks.
-constexpr int WALK_WIN = 1032;
+// Per warp two arrays of `win` words, win = min(B + 12, WALK_WIN) for the
+// level (dynamic shared memory, so that levels with short segments keep many
+// warps resident).
+constexpr int WALK_WIN = 1040;
+__host__ __device__ inline int walk_win(int B) { return B + 12 < WALK_WIN ? B + 12 : WALK_WIN; }
 
 __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes)
 {
-    __shared__ int32_t win_r[4][WALK_WIN], win_c[4][WALK_WIN];
+    extern __shared__ int32_t walk_smem[];
     if (*A.bad) return;
     const int lane = threadIdx.x & 31;
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -828,51 +836,100 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
     }
     (void)G;
     // The segment walks at most B + 1 steps, each one row up or one column
-    // right: rows [dr - B - 2, dr] and columns [dc - 1, dc + B + 1] cover it.
-    // The warp stages them (coalesced) so that lane 0 walks in shared memory.
+    // right, and reads words up to two steps ahead: rows [dr - B - 6, dr] and
+    // columns [dc - 1, dc + B + 5] cover it.  The warp stages them (coalesced) so that
+    // lane 0 walks in shared memory.
     const int wi = threadIdx.x >> 5;
-    const int rb = max(0, dr - B - 2), nr = min(max(dr - rb + 1, 0), WALK_WIN);
-    const int cb = max(0, dc - 1), nc = min(max(min(s, dc + B + 2) - cb, 0), WALK_WIN);
-    for (int t = lane; t < nr; t += 32) win_r[wi][t] = A.C[o + rb + t] | (A.H[o + rb + t] ? INT_MIN : 0);
-    for (int t = lane; t < nc; t += 32) win_c[wi][t] = A.R[o + cb + t] | (A.HC[o + cb + t] ? INT_MIN : 0);
+    const int win = walk_win(B);
+    int32_t *wr_s = walk_smem + size_t(wi) * 2 * win, *wc_s = wr_s + win;
+    const int rb = max(0, dr - B - 6), nr = min(max(dr - rb + 1, 0), win);
+    const int cb = max(0, dc - 1), nc = min(max(min(s, dc + B + 6) - cb, 0), win);
+    for (int t = lane; t < nr; t += 32) wr_s[t] = A.C[o + rb + t] | (A.H[o + rb + t] ? INT_MIN : 0);
+    for (int t = lane; t < nc; t += 32) wc_s[t] = A.R[o + cb + t] | (A.HC[o + cb + t] ? INT_MIN : 0);
     __syncwarp();
     if (lane != 0) return;
     // Outside the window (B > WALK_WIN - 8 only) the walk reads global memory.
-    auto rinc = [&](int r, int c) {
-        const unsigned t = unsigned(r - rb);
-        if (t < unsigned(nr)) {
-            const int w = win_r[wi][t];
-            const int cc = w & INT_MAX;
-            return w < 0 ? int(cc < c) : int(cc >= c);
+    const int32_t *wr = wr_s, *wc = wc_s;
+    ant_walk(
+        dr, dc, delta, s, E + B,
+        [&](int r) {
+            const unsigned t = unsigned(r - rb);
+            return t < unsigned(nr) ? wr[t] : (A.C[o + r] | (A.H[o + r] ? INT_MIN : 0));
+        },
+        [&](int c) {
+            const unsigned t = unsigned(c - cb);
+            return t < unsigned(nc) ? wc[t] : (A.R[o + c] | (A.HC[o + c] ? INT_MIN : 0));
+        },
+        [&](int r, int c) { A.res[o + r] = c; });
+}
+
+// Levels with short segments (B <= WALK_LANE_B) have many segments: one
+// lane per segment, all steps straight from global memory (L2), so that a
+// warp advances 32 walks at once instead of one.
+constexpr int WALK_LANE_B = 256;
+
+__device__ int delta_at_lane(const SegArgs &A, const int32_t *T, int o, int r, int c)
+{
+    const int i0 = r / A.B, j0 = c / A.B;
+    const int r0 = i0 * A.B, c0 = j0 * A.B;
+    int acc = T[i0 * A.stride + j0];
+    for (int rr = r0; rr < r; ++rr) acc += rowinc(A, o, rr, c0);
+    for (int cc = c0; cc < c; ++cc) acc += colinc(A, o, cc, r);
+    return acc;
+}
+
+__global__ void __launch_bounds__(256) walk_lanes_kernel(SegArgs A, int nodes)
+{
+    if (*A.bad) return;
+    const long gid = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (gid >= long(nodes) * A.nseg) return;
+    const int nd = int(gid / A.nseg), q = int(gid % A.nseg);
+    int o, s;
+    node_by_index(nd, A.level, A.k, o, s);
+    if (s <= 1) return;
+    const int B = A.B;
+    const int32_t *T = A.T + size_t(nd) * A.stride * A.stride;
+    const int jmin = -((s + B - 1) / B);
+    const int E = (jmin + q) * B;
+    const int e0 = -(s - 1);
+    if (E > s || E + B < e0) return;
+    int dr, dc, delta;
+    if (E < e0) {
+        dr = s - 1;
+        dc = 0;
+        delta = A.H[o + s - 1] ? 0 : -1;
+    } else {
+        const int rlo = max(0, -E), rhi = min(s, s - E);
+        if (rlo > rhi) return;
+        const int jj = E / B;
+        const int ilo = rlo / B, ihi = rhi / B;
+        int lo_i = ilo, hi_i = ihi + 1;
+        while (lo_i < hi_i) {
+            const int mid = (lo_i + hi_i) >> 1;
+            if (T[mid * A.stride + mid + jj] >= 0) hi_i = mid;
+            else lo_i = mid + 1;
         }
-        return rowinc(A, o, r, c);
-    };
-    auto cinc = [&](int c, int r) {
-        const unsigned t = unsigned(c - cb);
-        if (t < unsigned(nc)) {
-            const int w = win_c[wi][t];
-            const int rr = w & INT_MAX;
-            return w < 0 ? int(rr < r) : int(rr >= r);
+        int rstar = rlo;
+        if (lo_i != ilo) {
+            int dval = T[(lo_i - 1) * A.stride + (lo_i - 1) + jj];
+            const int rend = min(lo_i * B, rhi);
+            rstar = rhi + 1;
+            for (int r = (lo_i - 1) * B; r < rend; ++r) {
+                dval += colinc(A, o, r + E, r) + rowinc(A, o, r, r + E + 1);
+                if (dval >= 0) {
+                    rstar = r + 1;
+                    break;
+                }
+            }
         }
-        return colinc(A, o, c, r);
-    };
-    const int last = E + B;
-    while (dr >= 0 && dc <= s && dc - dr <= last) {
-        if (dc > 0) {
-            const int dl = delta - cinc(dc - 1, dr);
-            const int dd = delta + rinc(dr, dc);
-            if (dl < 0 && dd > 0) A.res[o + dr] = dc - 1;
-        }
-        if (delta < 0) {
-            if (dc + 1 <= s) delta += cinc(dc, dr);
-            ++dc;
-        } else if (delta == 0) {
-            if (dr - 1 >= 0) delta -= rinc(dr - 1, dc);
-            --dr;
-        } else {
-            break;
-        }
+        dr = rstar - 1;
+        dc = rstar + E;
+        if (dr < 0 || dc > s) return;
+        delta = delta_at_lane(A, T, o, dr, dc);
     }
+    ant_walk(
+        dr, dc, delta, s, E + B, [&](int r) { return A.C[o + r] | (A.H[o + r] ? INT_MIN : 0); },
+        [&](int c) { return A.R[o + c] | (A.HC[o + c] ? INT_MIN : 0); }, [&](int r, int c) { A.res[o + r] = c; });
 }
 
 // ---------------------------------------------------------------------------
@@ -1239,7 +1296,12 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         const int nseg = 2 * ((smax + B - 1) / B) + 2;
         SegArgs SA{C, H, Rr, HC, tab_hi, res + kk * size_t(l), k, l, B, stride, nseg, bad};
         const long warps = long(nodes) * nseg;
-        walk_segments_kernel<<<int((warps * 32 + 127) / 128), 128, 0, st>>>(SA, nodes);
+        if (B <= WALK_LANE_B) {
+            walk_lanes_kernel<<<int((warps + 255) / 256), 256, 0, st>>>(SA, nodes);
+        } else {
+            const size_t wsm = size_t(4) * 2 * walk_win(B) * sizeof(int32_t);
+            walk_segments_kernel<<<int((warps * 32 + 127) / 128), 128, wsm, st>>>(SA, nodes);
+        }
     }
     AssembleArgs A{P, P_c2r, Q, res, map_row, map_col, out, p, q, k, row_glue, bad};
     assemble_kernel<<<blocks_for(long(p) + q + k, 256), 256, 0, st>>>(A);

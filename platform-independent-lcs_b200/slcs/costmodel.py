@@ -168,12 +168,22 @@ class CostModel:
 _MODEL = None
 
 
-def choose(batch) -> Optional[Config]:
-    """The model's variant for a batch, or None when no model is installed."""
+def installed_model() -> Optional[CostModel]:
     global _MODEL
     if _MODEL is None:
         _MODEL = CostModel.load() or False
-    if not _MODEL:
+    return _MODEL or None
+
+
+def ranking(batch) -> Optional[np.ndarray]:
+    """Variant indices, fastest predicted first (None without a model)."""
+    model = installed_model()
+    if model is None:
         return None
-    i = int(_MODEL.choose_index(batch_features(batch)[None, :])[0])
-    return variant_config(i)
+    return np.argsort(model.predict(batch_features(batch)[None, :])[0], kind="stable")
+
+
+def choose(batch) -> Optional[Config]:
+    """The model's variant for a batch, or None when no model is installed."""
+    r = ranking(batch)
+    return None if r is None else variant_config(int(r[0]))

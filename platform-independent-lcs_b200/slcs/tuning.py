@@ -23,15 +23,31 @@ def heuristic_batch_config(batch) -> Config:
     return Config.make(use_graph=1)
 
 
-def choose_batch_config(batch):
+def choose_batch_config(batch, timer=None, top: int = 3):
+    """(config, how it was chosen, details).
+
+    With a trained cost model, its first choice -- or, when `timer` is given
+    (a callable that times one run of a Config on the actual batch), the
+    fastest of its `top` best-ranked variants, measured: the model prunes the
+    search from every variant to a few.  Without a model, the fixed
+    heuristic."""
     try:
         from . import costmodel
-        cfg = costmodel.choose(batch)
-        if cfg is not None:
-            return cfg, "cost_model"
+        order = costmodel.ranking(batch)
     except Exception:
-        pass
-    return heuristic_batch_config(batch), "heuristic"
+        order = None
+    if order is None:
+        return heuristic_batch_config(batch), "heuristic", {}
+    names = [costmodel.VARIANTS[int(i)]["name"] for i in order[:top]]
+    if timer is None:
+        return costmodel.variant_config(int(order[0])), "cost_model", {"model_choice": names[0]}
+    times = {}
+    for i in order[:top]:
+        times[costmodel.VARIANTS[int(i)]["name"]] = float(timer(costmodel.variant_config(int(i))))
+    best = min(times, key=times.get)
+    idx = [v["name"] for v in costmodel.VARIANTS].index(best)
+    return (costmodel.variant_config(idx), f"cost_model_top{top}_timed",
+            {"model_choice": names[0], "candidates_ms": times, "chosen": best})
 
 
 def per_pair_loop(batch, a_d, b_d, out, stream_handle, limit=None):
