@@ -4,6 +4,7 @@
 // workspace management, batch plans with optional CUDA-graph replay, and the
 // synchronous host-pointer wrappers.  All combing runs in comb.cu.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -73,6 +74,26 @@ int pick_tile_m(const slcs_config *cfg, int32_t m_typical, int64_t total_cells)
     if (m_typical <= 64) return 2;
     if (m_typical <= 128) return 4;
     return 8;
+}
+
+// Column strips for one pair when nothing is configured, fitted to B200
+// timings of uniform {0..3} pairs.  One wavefront keeps few warps busy below
+// about 2^19 rows (stripe t starts 32 column blocks after stripe t-1), while
+// every strip adds a braid product with overlap m.  About n / sqrt(4096 m)
+// strips (a power of two, rounded up from 2^(k+0.45); 1..64 strips of at
+// least 4096 columns) balance the two; pairs of 2^17 and of 2^18 rows and
+// more take at most 4 and 2 strips.
+int auto_strips(int32_t m, int32_t n)
+{
+    if (m <= 0 || n < 8192 || m >= (1 << 19)) return 1;
+    const double base = double(n) / std::sqrt(4096.0 * double(m));
+    int S = base <= 1.0 ? 1 : 1 << int(std::floor(std::log2(base) + 0.55));
+    if (n >= 32768) S = std::max(S, 2);
+    if (m >= (1 << 17)) S = std::min(S, 4);
+    if (m >= (1 << 18)) S = std::min(S, 2);
+    S = std::min(S, 64);
+    while (S > 1 && n / S < 4096) S /= 2;
+    return S;
 }
 
 // 16 rows per lane leave room for 8 warps per block; the smaller tiles run 4.
@@ -329,6 +350,18 @@ slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_
     if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
     (void)sm_count(); // per-device set-up (memory pool) before the first allocation
     if (cfg && cfg->algo == SLCS_ALGO_STRIPS) return comb_strips(a, m, b, n, h_out, v_out, cfg, tm, pick_warps(cfg, tm), st);
+    if (!cfg || (cfg->algo == SLCS_ALGO_AUTO && cfg->tile_m == 0 && cfg->warps == 0 && cfg->strips == 0)) {
+        const int S = auto_strips(m, n);
+        if (S > 1) {
+            slcs_config c = cfg ? *cfg : slcs_config{};
+            c.algo = SLCS_ALGO_STRIPS;
+            c.strips = S;
+            c.tile_m = 16;
+            c.warps = 4;
+            if (c.braid_cutoff <= 0) c.braid_cutoff = 256;
+            return comb_strips(a, m, b, n, h_out, v_out, &c, 16, 4, st);
+        }
+    }
     const int32_t ntasks = stripes_of(m, tm);
     const size_t work_bytes = align_up(sizeof(int32_t) * (4 + size_t(ntasks)), 256);
     const size_t scr_bytes = sizeof(int32_t) * size_t(scratch_elems(m, n, tm));

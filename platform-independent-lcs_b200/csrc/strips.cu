@@ -13,6 +13,7 @@
 // permutations multiplied) at strip granularity; it is also the per-GPU unit
 // of the multi-GPU split, where each rank combs one strip.
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "braid.cuh"
@@ -39,6 +40,30 @@ __global__ void perm_to_strands_kernel(const int32_t *__restrict__ r2c, int32_t 
 }
 
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Products of one tree level are independent: they run side by side on a
+// small pool of streams per device (created once, never destroyed), each
+// with its own braid workspace, forked from and joined back to the caller's
+// stream with events.
+constexpr int MAX_SIDE = 8;
+std::mutex g_side_mu;
+std::vector<cudaStream_t> g_side[64];
+
+slcs_status side_streams(int count, cudaStream_t *out)
+{
+    int dev = 0;
+    SLCS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(SLCS_ERR_UNSUPPORTED, "device index out of range");
+    std::lock_guard<std::mutex> g(g_side_mu);
+    auto &v = g_side[dev];
+    while (int(v.size()) < count) {
+        cudaStream_t t = nullptr;
+        SLCS_CUDA(cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
+        v.push_back(t);
+    }
+    for (int i = 0; i < count; ++i) out[i] = v[size_t(i)];
+    return SLCS_OK;
+}
 
 } // namespace
 
@@ -111,7 +136,9 @@ slcs_status comb_strips(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n
     const size_t o_x = align256(o_scr + sizeof(int32_t) * size_t(scr_elems) + 16);
     const size_t o_y = align256(o_x + sizeof(int32_t) * size_t(total));
     const size_t o_braid = align256(o_y + sizeof(int32_t) * size_t(total));
-    const size_t bytes = o_braid + braid_bytes;
+    const int par = std::max(1, std::min(MAX_SIDE, S / 2)); // products of a level in flight
+    braid_bytes = align256(braid_bytes);
+    const size_t bytes = o_braid + braid_bytes * size_t(par);
     char *ws = nullptr;
     SLCS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&ws), bytes, st));
     slcs_status s = SLCS_OK;
@@ -154,17 +181,32 @@ slcs_status comb_strips(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n
         s = launch_strands_to_perm(X + off, m, X + off + m, w[size_t(k)], Y + off, nullptr, st);
         level.push_back({Y + off, int64_t(m) + w[size_t(k)]});
     }
-    // Balanced merge tree, ping-ponging between Y and X.
+    // Balanced merge tree, ping-ponging between Y and X; the products of a
+    // level run on `par` side streams.
     int32_t *dst = X;
-    void *bws = ws + o_braid;
+    cudaStream_t side[MAX_SIDE] = {};
+    if (s == SLCS_OK && S > 1) s = side_streams(par, side);
+    cudaEvent_t fork = nullptr, join[MAX_SIDE] = {};
+    if (s == SLCS_OK && S > 1) {
+        cu(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
+        for (int j = 0; j < par; ++j) cu(cudaEventCreateWithFlags(&join[j], cudaEventDisableTiming), "event");
+    }
     while (s == SLCS_OK && level.size() > 1) {
         std::vector<Perm> next;
         int64_t off = 0;
+        cu(cudaEventRecord(fork, st), "fork");
+        int used = 0;
         for (size_t i = 0; i < level.size() && s == SLCS_OK; i += 2) {
             if (i + 1 < level.size()) {
+                const int j = int((i / 2) % size_t(par));
+                if (j >= used) {
+                    cu(cudaStreamWaitEvent(side[j], fork, 0), "fork wait");
+                    used = j + 1;
+                }
                 const int64_t size = level[i].size + level[i + 1].size - m;
-                s = launch_braid(level[i].p, int(level[i].size), level[i + 1].p, int(level[i + 1].size), m, false,
-                                 dst + off, cutoff, bws, braid_bytes, st);
+                if (s == SLCS_OK)
+                    s = launch_braid(level[i].p, int(level[i].size), level[i + 1].p, int(level[i + 1].size), m, false,
+                                     dst + off, cutoff, ws + o_braid + braid_bytes * size_t(j), braid_bytes, side[j]);
                 next.push_back({dst + off, size});
                 off += size;
             } else {
@@ -175,9 +217,16 @@ slcs_status comb_strips(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n
                 off += level[i].size;
             }
         }
+        for (int j = 0; j < used; ++j) {
+            cu(cudaEventRecord(join[j], side[j]), "join");
+            cu(cudaStreamWaitEvent(st, join[j], 0), "join wait");
+        }
         level.swap(next);
         dst = (dst == X) ? Y : X;
     }
+    if (fork) cudaEventDestroy(fork);
+    for (int j = 0; j < par; ++j)
+        if (join[j]) cudaEventDestroy(join[j]);
     if (s == SLCS_OK) s = perm_to_strands(level[0].p, m, n, h_out, v_out, st);
     cudaFreeAsync(ws, st);
     return s;

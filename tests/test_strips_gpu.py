@@ -64,3 +64,17 @@ def test_strips_pair_131072_mutated(cuda):
     c2r = c2r.cpu().numpy()
     assert hashlib.sha256(c2r.tobytes()).hexdigest() == g["sha256_col_to_row"]
     assert slcs.permutation_hash(c2r) == g["hash"]
+
+
+@pytest.mark.parametrize("m,n", [(600, 300000), (20000, 70000), (5000, 5000)])
+def test_default_rule_picks_strips_and_matches(cuda, m, n):
+    """The default configuration combs wide and mid-size pairs as strips
+    (many strips for a short, wide pair); strands equal the oracle's."""
+    rng = np.random.default_rng(m + n)
+    a = rng.integers(0, 4, m, dtype=np.uint8)
+    b = rng.integers(0, 4, n, dtype=np.uint8)
+    h, v = slcs.comb_pair(_dev(a, cuda), _dev(b, cuda))
+    slcs.device_status(0)
+    eh, ev = O.comb(a, b)
+    np.testing.assert_array_equal(h.cpu().numpy(), eh)
+    np.testing.assert_array_equal(v.cpu().numpy(), ev)
