@@ -3,6 +3,7 @@
     python -m slcs.profile_case batch [npairs]     # one batch launch (read/window pairs)
     python -m slcs.profile_case pair  [length]     # one square uniform pair
     python -m slcs.profile_case braid [k] [cutoff] # one staggered product of overlap k
+    python -m slcs.profile_case default 131072     # the 131072 mutated pair, default configuration
 
 Each case runs one warm-up launch and then the launch to capture, and checks
 the device status word; it holds a few hundred MB on the device at most.
@@ -42,6 +43,14 @@ def main():
         cfg = slcs.Config.make(tile_m=tm or 16, wait_ms=600000)
         for _ in range(2):
             slcs.comb_pair(a, b, cfg=cfg, out=out)
+        torch.cuda.synchronize()
+    elif kind == "default":
+        a_h, b_h = W.pair_131072_mutated() if (size or 131072) == 131072 else W.pair_1m()
+        a = torch.from_numpy(a_h).to(dev)
+        b = torch.from_numpy(b_h).to(dev)
+        out = torch.empty(len(a_h) + len(b_h), dtype=torch.int32, device=dev)
+        for _ in range(2):
+            slcs.comb_pair(a, b, cfg=slcs.Config.make(wait_ms=600000), out=out)
         torch.cuda.synchronize()
     elif kind == "braid":
         k = size or (1 << 18)
