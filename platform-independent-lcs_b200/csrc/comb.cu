@@ -130,28 +130,10 @@ __device__ __forceinline__ void comb_stripe(const CombLaunch &L, const PairDev &
 #pragma unroll
     for (int j = 0; j < TN; ++j) vc[j] = INT_MAX;
 
-    // The four symbols of a column block as one word (0 past the end; those
-    // columns are masked below).  Words are loaded two steps before use so
-    // that the L2 latency hides behind the cells of the steps between.
-    auto fetch = [&](int bk) -> uint32_t {
-        if (unsigned(bk) >= unsigned(nb)) return 0u;
-        const int c = bk * TN;
-        if (b_aligned && c + TN <= n) return __ldg(reinterpret_cast<const uint32_t *>(b + c));
-        uint32_t w = 0;
-#pragma unroll
-        for (int j = 0; j < TN; ++j)
-            if (c + j < n) w |= uint32_t(__ldg(b + c + j)) << (8 * j);
-        return w;
-    };
-    uint32_t w0 = fetch(-lane), w1 = fetch(1 - lane);
-
     const int steps = nb + 31;
     for (int t = 0; t < steps; ++t) {
         const int blk = t - lane;
         const bool act = unsigned(blk) < unsigned(nb);
-        const uint32_t wcur = w0;
-        w0 = w1;
-        w1 = fetch(blk + 2);
 
         int vi[TN];
 #pragma unroll
@@ -189,8 +171,20 @@ __device__ __forceinline__ void comb_stripe(const CombLaunch &L, const PairDev &
         }
 
         int bs[TN];
+        if (act) {
+            const int c = blk * TN;
+            if (b_aligned && c + TN <= n) {
+                const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(b + c));
 #pragma unroll
-        for (int j = 0; j < TN; ++j) bs[j] = (act && blk * TN + j < n) ? int((wcur >> (8 * j)) & 0xffu) : -2;
+                for (int j = 0; j < TN; ++j) bs[j] = int((w >> (8 * j)) & 0xffu);
+            } else {
+#pragma unroll
+                for (int j = 0; j < TN; ++j) bs[j] = (c + j < n) ? int(__ldg(b + c + j)) : -2;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < TN; ++j) bs[j] = -2;
+        }
 
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
