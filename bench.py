@@ -292,7 +292,8 @@ def main():
 
     extras = {}
     if not args.no_extras and rank == 0:
-        extras = tuning.secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev)
+        extras = tuning.secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev,
+                                               sampler=lambda: ClockSampler(local))
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

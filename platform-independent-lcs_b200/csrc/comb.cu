@@ -670,8 +670,15 @@ slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_o
         }
     }
     if (stream == PREPARE_ONLY) return SLCS_OK;
-    const long want = (long(L.ntasks) + WARPS - 1) / WARPS;
-    long grid = long(sm_count()) * occ;
+    // One warp per stripe at most; beyond one block per SM the grid is rounded
+    // up to a multiple of the SM count (surplus warps find no ticket and
+    // exit), so that every SM hosts the same number of warps.  With 2048
+    // stripes of 8-warp blocks, 256 blocks left 40 SMs at half load and the
+    // stripes on the full SMs set the pace of the whole wavefront.
+    const long sms = sm_count();
+    long want = (long(L.ntasks) + WARPS - 1) / WARPS;
+    if (want > sms) want = (want + sms - 1) / sms * sms;
+    long grid = sms * occ;
     if (want < grid) grid = want;
     if (grid < 1) grid = 1;
     comb_wavefront_kernel<TM, WARPS><<<int(grid), WARPS * 32, 0, stream>>>(L);

@@ -64,7 +64,10 @@ def per_pair_loop(batch, a_d, b_d, out, stream_handle, limit=None):
                                stream_handle))
 
 
-def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev):
+def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev, sampler=None):
+    """Plain per-pair loop, the 2^20 pair (best of 3 runs, with the SM clocks
+    sampled while it runs when `sampler` -- a context-manager factory with a
+    summary() -- is given), strips and braid products."""
     import torch
     res = {}
     st = torch.cuda.current_stream()
@@ -91,11 +94,19 @@ def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev):
     cfg = Config.make()  # default rule: 16 rows per lane, 8 warps per block at this height
     comb_pair(ad, bd, cfg=cfg, out=o)
     torch.cuda.synchronize()
-    e0.record(st)
-    comb_pair(ad, bd, cfg=cfg, out=o)
-    e1.record(st)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    runs = []
+    smp = sampler() if sampler else None
+    if smp:
+        smp.__enter__()
+    for _ in range(3):
+        e0.record(st)
+        comb_pair(ad, bd, cfg=cfg, out=o)
+        e1.record(st)
+        torch.cuda.synchronize()
+        runs.append(e0.elapsed_time(e1))
+    if smp:
+        smp.__exit__(None, None, None)
+    ms = min(runs)
     cells = len(a) * len(b)
     g = cells / (ms * 1e-3) / 1e9
     _, c2r = strands_to_permutation(o[:len(a)], o[len(a):])
@@ -108,7 +119,8 @@ def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev):
     res["long_pair"] = {"workload": "pair_1M (1048576 x 1048576, uniform {0..3})", "ms": ms, "gcups": g,
                         "roofline_frac": g / roof_gcups, "hash": hv,
                         "bitexact_vs_reference": (hv == gold) if gold is not None else None,
-                        "variant": {"tile_m": 16, "warps": 8}}
+                        "variant": {"tile_m": 16, "warps": 8}, "runs_ms": runs,
+                        "clocks": smp.summary() if smp else None}
     res.update(strips_and_braid(ad, bd, o, gold, dev))
     return res
 
