@@ -4,6 +4,8 @@ training data.  Also scores a variant chooser by its regret against exhaustive
 tuning.
 
     python -m slcs.autotune collect --train 8000 --test 2000 --out DB.npz
+    python -m slcs.autotune collect --train 8000 --train-start 2400 ...   # only shapes 2400.. of the sample
+    python -m slcs.autotune merge A.npz B.npz --out DB.npz                # concatenate collections
     python -m slcs.autotune fit DB.npz           # trains on the GPU, writes slcs/data/costmodel.json
 
 Shapes follow the sweep definition (slcs.workloads.sweep_shapes): m, n
@@ -146,24 +148,47 @@ def report(model: CM.CostModel, feats, times) -> dict:
             "plain": regret(times, np.full(len(times), CM.PLAIN))}
 
 
+def merge(parts, out):
+    """Concatenate collections of the same variant list (train and test parts)."""
+    dbs = [np.load(p) for p in parts]
+    names = [list(d["variants"]) for d in dbs]
+    if any(n != names[0] for n in names):
+        raise SystemExit("collections timed different variant lists")
+    res = {"variants": dbs[0]["variants"]}
+    for split in ("train", "test"):
+        for key in ("X", "ms", "agree", "shape"):
+            k = f"{split}_{key}"
+            res[k] = np.concatenate([d[k] for d in dbs if k in d.files and len(d[k])])
+    np.savez_compressed(out, **res)
+    print({k: v.shape for k, v in res.items()})
+
+
 def main():
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
     c = sub.add_parser("collect")
     c.add_argument("--train", type=int, default=8000)
     c.add_argument("--test", type=int, default=2000)
+    c.add_argument("--train-start", type=int, default=0, help="first training shape to time (sample prefix is stable)")
+    c.add_argument("--test-start", type=int, default=0)
     c.add_argument("--cell-cap", type=float, default=2e8)
     c.add_argument("--out", default=os.path.join(HERE, "data", "timings.npz"))
+    mg = sub.add_parser("merge")
+    mg.add_argument("parts", nargs="+")
+    mg.add_argument("--out", required=True)
     f = sub.add_parser("fit")
     f.add_argument("db", nargs="?", default=os.path.join(HERE, "data", "timings.npz"))
     f.add_argument("--epochs", type=int, default=3000)
     f.add_argument("--lr", type=float, default=3e-3)
     args = ap.parse_args()
+    if args.cmd == "merge":
+        merge(args.parts, args.out)
+        return
     import torch
     dev = torch.device("cuda:0")
     if args.cmd == "collect":
-        train = W.sweep_shapes(args.train, seed=11, cell_cap=args.cell_cap)
-        test = W.sweep_shapes(args.test, seed=12, cell_cap=args.cell_cap)
+        train = W.sweep_shapes(args.train, seed=11, cell_cap=args.cell_cap)[args.train_start:]
+        test = W.sweep_shapes(args.test, seed=12, cell_cap=args.cell_cap)[args.test_start:]
         out = {}
         for name, shapes in (("train", train), ("test", test)):
             t0 = time.time()
