@@ -189,6 +189,17 @@ SLCS_API slcs_status slcs_strands_to_permutation(const int32_t *h, int32_t m, co
 SLCS_API slcs_status slcs_permutation_to_strands(const int32_t *row_to_col, int32_t m, int32_t n, int32_t *h,
                                                  int32_t *v, void *stream);
 
+/* Semi-local string-substring LCS from the strands of one comb: for each
+ * query q, llcs_out[q] = LLCS(a, b[begin[q], end[q])), computed as
+ * (end - begin) - #{k in [begin, end) : v_strands[k] >= m + begin}.  The
+ * reference computes the strands for exactly these answers and checks the
+ * whole-string one against its prefix DP (src/lcs_reference.hpp:71-132).
+ * v_strands (n), begin, end and llcs_out (nq) are device arrays; a query
+ * outside 0 <= begin <= end <= n gets -1 and slcs_device_status() reports
+ * SLCS_ERR_INVALID. */
+SLCS_API slcs_status slcs_substring_llcs(const int32_t *v_strands, int32_t m, int32_t n, const int32_t *begin,
+                                         const int32_t *end, int32_t nq, int32_t *llcs_out, void *stream);
+
 /* PermutationMatrix::hash (src/permutation_matrix.hpp:192-203) of a host
  * col_to_row array, with the reference's signed 64-bit wrap-around. */
 SLCS_API int64_t slcs_permutation_hash(const int32_t *col_to_row, int32_t size);

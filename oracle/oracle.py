@@ -253,3 +253,14 @@ def mt19937_binary(size: int, seed: int) -> np.ndarray:
     bg = np.random.RandomState(seed)._bit_generator
     raw = bg.random_raw(size)
     return (raw & 1).astype(np.uint8)
+
+
+def substring_llcs(v, m: int, begin, end):
+    """LLCS(a, b[i, j)) = (j - i) - #{k in [i, j) : v[k] >= m + i} from the
+    v strands of the comb of (a, b) (the semi-local string-substring solution;
+    checked against the DP of prefix_llcs in the tests)."""
+    v = np.asarray(v)
+    out = np.empty(len(begin), np.int64)
+    for q, (i, j) in enumerate(zip(begin, end)):
+        out[q] = (j - i) - int(np.count_nonzero(v[i:j] >= m + i))
+    return out

@@ -14,6 +14,7 @@
 
 #include "braid.cuh"
 #include "comb.cuh"
+#include "queries.cuh"
 #include "strips.cuh"
 
 namespace slcs {
@@ -874,6 +875,16 @@ slcs_status slcs_strands_to_permutation(const int32_t *h, int32_t m, const int32
     if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
     if ((m > 0 && !h) || (n > 0 && !v)) return fail(SLCS_ERR_INVALID, "null strands");
     return launch_strands_to_perm(h, m, v, n, row_to_col, col_to_row, static_cast<cudaStream_t>(stream));
+}
+
+slcs_status slcs_substring_llcs(const int32_t *v_strands, int32_t m, int32_t n, const int32_t *begin,
+                                const int32_t *end, int32_t nq, int32_t *llcs_out, void *stream)
+{
+    if (m < 0 || n < 0 || nq < 0) return fail(SLCS_ERR_INVALID, "m, n and nq must be >= 0");
+    if (int64_t(m) + n > INT32_MAX) return fail(SLCS_ERR_RANGE, "m+n exceeds int32 strand ids");
+    if (nq > 0 && (!begin || !end || !llcs_out || (n > 0 && !v_strands)))
+        return fail(SLCS_ERR_INVALID, "null strands or query arrays");
+    return launch_substring_llcs(v_strands, m, n, begin, end, nq, llcs_out, static_cast<cudaStream_t>(stream));
 }
 
 slcs_status slcs_permutation_to_strands(const int32_t *row_to_col, int32_t m, int32_t n, int32_t *h, int32_t *v,

@@ -92,6 +92,7 @@ def lib():
         L.slcs_batch_plan_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
         L.slcs_strands_to_permutation.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, _vp]
         L.slcs_permutation_to_strands.argtypes = [_vp, _i32, _i32, _vp, _vp, _vp]
+        L.slcs_substring_llcs.argtypes = [_vp, _i32, _i32, _vp, _vp, _i32, _vp, _vp]
         L.slcs_permutation_hash.argtypes = [_vp, _i32]
         L.slcs_permutation_hash.restype = _i64
         L.slcs_probe_int_rates.argtypes = [_i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _vp]
@@ -246,6 +247,17 @@ def permutation_to_strands(r2c, m: int, stream=None):
     check(lib().slcs_permutation_to_strands(_dptr(r2c), int(m), n, _dptr(out), _dptr(out) + 4 * int(m) if n else 0,
                                             _stream(stream)))
     return out[:m], out[m:]
+
+
+def substring_llcs(v, m: int, begin, end, stream=None):
+    """LLCS(a, b[begin[q], end[q])) for every query q, from the v strands of
+    the comb of (a, b) (int32 CUDA tensors; -1 for a query out of range)."""
+    import torch
+    nq = int(begin.numel())
+    out = torch.empty(nq, dtype=torch.int32, device=v.device)
+    check(lib().slcs_substring_llcs(_dptr(v), int(m), int(v.numel()), _dptr(begin), _dptr(end), nq, _dptr(out),
+                                    _stream(stream)))
+    return out
 
 
 def permutation_hash(col_to_row: np.ndarray) -> int:

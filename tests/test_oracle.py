@@ -136,3 +136,18 @@ def test_permutation_is_full():
     r2c, c2r = O.from_strands(*O.comb(a, b))
     assert sorted(r2c.tolist()) == list(range(821))
     np.testing.assert_array_equal(c2r[r2c], np.arange(821))
+
+
+def test_substring_llcs_formula_matches_dp():
+    """LLCS(a, b[i, j)) from the strands equals the DP for every substring."""
+    rng = np.random.default_rng(21)
+    for _ in range(25):
+        m, n = int(rng.integers(1, 30)), int(rng.integers(1, 30))
+        s = int(rng.choice([2, 3, 4]))
+        a = rng.integers(0, s, m, dtype=np.uint8)
+        b = rng.integers(0, s, n, dtype=np.uint8)
+        _, v = O.comb(a, b)
+        qi, qj = zip(*[(i, j) for i in range(n + 1) for j in range(i, n + 1)])
+        got = O.substring_llcs(v, m, qi, qj)
+        want = [O.prefix_llcs(a, b[i:j]) if j > i else 0 for i, j in zip(qi, qj)]
+        np.testing.assert_array_equal(got, want)
