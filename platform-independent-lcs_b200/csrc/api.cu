@@ -240,6 +240,17 @@ struct slcs_batch_plan {
     // Device staging of slcs_batch_plan_run_host, grown on demand.
     char *h_stage = nullptr;
     size_t h_stage_bytes = 0;
+    // Host runs of large batches: the pairs in index order cut into chunks
+    // with disjoint byte ranges of a, b and out, one sub-plan and one stream
+    // each, so that one chunk's copies overlap another chunk's combing.
+    struct Chunk {
+        slcs_batch_plan *plan = nullptr;
+        int64_t a_lo = 0, a_hi = 0, b_lo = 0, b_hi = 0, o_lo = 0, o_hi = 0;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t done = nullptr;
+    };
+    std::vector<Chunk> chunks;
+    cudaEvent_t chunk_start = nullptr;
 
     CombLaunch launch(const uint8_t *a, const uint8_t *b, int32_t *out) const
     {
@@ -447,8 +458,97 @@ slcs_status slcs_comb_pair_host(const uint8_t *a, int32_t m, const uint8_t *b, i
     return slcs_device_status(dev, 1);
 }
 
+static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_desc *pairs, int32_t npairs,
+                                    const slcs_config *cfg);
+static void plan_add_chunks(slcs_batch_plan *P, const slcs_pair_desc *pairs, int32_t npairs, const slcs_config *cfg);
+
 slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_desc *pairs, int32_t npairs,
                                    const slcs_config *cfg)
+{
+    slcs_status s = plan_create_impl(plan_out, pairs, npairs, cfg);
+    if (s == SLCS_OK) plan_add_chunks(*plan_out, pairs, npairs, cfg);
+    return s;
+}
+
+// Chunks for host runs (an optimisation only: without them run_host copies
+// everything in, combs, and copies everything out).  Made for batches of at
+// least CHUNK_MIN_PAIRS pairs whose chunks' byte ranges do not overlap.
+static constexpr int HOST_CHUNKS = 4;
+static constexpr int32_t CHUNK_MIN_PAIRS = 8192;
+
+static void plan_add_chunks(slcs_batch_plan *P, const slcs_pair_desc *pairs, int32_t npairs, const slcs_config *cfg)
+{
+    if (npairs < CHUNK_MIN_PAIRS) return;
+    int64_t cells = 0;
+    for (int32_t p = 0; p < npairs; ++p) cells += int64_t(pairs[p].m) * pairs[p].n;
+    std::vector<slcs_batch_plan::Chunk> ch;
+    int32_t p0 = 0;
+    int64_t acc = 0;
+    for (int c = 0; c < HOST_CHUNKS && p0 < npairs; ++c) {
+        int32_t p1 = p0;
+        const int64_t target = cells * (c + 1) / HOST_CHUNKS;
+        while (p1 < npairs && (acc < target || p1 == p0)) {
+            acc += int64_t(pairs[p1].m) * pairs[p1].n;
+            ++p1;
+        }
+        if (c == HOST_CHUNKS - 1) {
+            for (; p1 < npairs; ++p1) acc += int64_t(pairs[p1].m) * pairs[p1].n;
+        }
+        slcs_batch_plan::Chunk k;
+        k.a_lo = k.b_lo = k.o_lo = INT64_MAX;
+        for (int32_t p = p0; p < p1; ++p) {
+            const slcs_pair_desc &d = pairs[p];
+            k.a_lo = std::min(k.a_lo, d.a_offset);
+            k.a_hi = std::max(k.a_hi, d.a_offset + d.m);
+            k.b_lo = std::min(k.b_lo, d.b_offset);
+            k.b_hi = std::max(k.b_hi, d.b_offset + d.n);
+            k.o_lo = std::min(k.o_lo, d.out_offset);
+            k.o_hi = std::max(k.o_hi, d.out_offset + d.m + d.n);
+        }
+        // Sub-plan over the chunk's pairs (offsets stay global).
+        if (plan_create_impl(&k.plan, pairs + p0, p1 - p0, cfg) != SLCS_OK) {
+            for (auto &x : ch) slcs_batch_plan_destroy(x.plan);
+            if (k.plan) slcs_batch_plan_destroy(k.plan);
+            return;
+        }
+        ch.push_back(k);
+        p0 = p1;
+    }
+    // Ranges must not overlap (reads of one chunk may not see another's copy
+    // still in flight, writes must not race).
+    auto disjoint = [&](int64_t slcs_batch_plan::Chunk::*lo, int64_t slcs_batch_plan::Chunk::*hi) {
+        std::vector<std::pair<int64_t, int64_t>> r;
+        for (auto &x : ch) r.push_back({x.*lo, x.*hi});
+        std::sort(r.begin(), r.end());
+        for (size_t i = 1; i < r.size(); ++i)
+            if (r[i].first < r[i - 1].second) return false;
+        return true;
+    };
+    bool ok = ch.size() > 1 && disjoint(&slcs_batch_plan::Chunk::a_lo, &slcs_batch_plan::Chunk::a_hi) &&
+              disjoint(&slcs_batch_plan::Chunk::b_lo, &slcs_batch_plan::Chunk::b_hi) &&
+              disjoint(&slcs_batch_plan::Chunk::o_lo, &slcs_batch_plan::Chunk::o_hi);
+    for (auto &x : ch) {
+        if (!ok) break;
+        ok = cudaStreamCreateWithFlags(&x.stream, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&x.done, cudaEventDisableTiming) == cudaSuccess;
+    }
+    if (ok) ok = cudaEventCreateWithFlags(&P->chunk_start, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        for (auto &x : ch) {
+            slcs_batch_plan_destroy(x.plan);
+            if (x.stream) cudaStreamDestroy(x.stream);
+            if (x.done) cudaEventDestroy(x.done);
+        }
+        if (P->chunk_start) cudaEventDestroy(P->chunk_start);
+        P->chunk_start = nullptr;
+        return;
+    }
+    P->chunks = std::move(ch);
+}
+
+static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_desc *pairs, int32_t npairs,
+                                    const slcs_config *cfg)
 {
     if (!plan_out) return fail(SLCS_ERR_INVALID, "plan is null");
     *plan_out = nullptr;
@@ -785,6 +885,30 @@ slcs_status slcs_batch_plan_run_host(slcs_batch_plan *P, const uint8_t *a, int64
     uint8_t *da = reinterpret_cast<uint8_t *>(P->h_stage);
     uint8_t *db = reinterpret_cast<uint8_t *>(P->h_stage + ab);
     int32_t *dout = reinterpret_cast<int32_t *>(P->h_stage + ab + bb);
+    if (!P->chunks.empty()) {
+        // Each chunk on its own stream: copy its ranges in, comb, copy its
+        // strands out.  With pinned host buffers the copy engines move one
+        // chunk while another combs.
+        SLCS_CUDA(cudaEventRecord(P->chunk_start, st));
+        for (auto &k : P->chunks) {
+            SLCS_CUDA(cudaStreamWaitEvent(k.stream, P->chunk_start, 0));
+            if (k.a_hi > k.a_lo)
+                SLCS_CUDA(cudaMemcpyAsync(da + k.a_lo, a + k.a_lo, size_t(k.a_hi - k.a_lo), cudaMemcpyHostToDevice,
+                                          k.stream));
+            if (k.b_hi > k.b_lo)
+                SLCS_CUDA(cudaMemcpyAsync(db + k.b_lo, b + k.b_lo, size_t(k.b_hi - k.b_lo), cudaMemcpyHostToDevice,
+                                          k.stream));
+            slcs_status s = slcs_batch_plan_run(k.plan, da, db, dout, k.stream);
+            if (s != SLCS_OK) return s;
+            if (k.o_hi > k.o_lo)
+                SLCS_CUDA(cudaMemcpyAsync(out + k.o_lo, dout + k.o_lo, sizeof(int32_t) * size_t(k.o_hi - k.o_lo),
+                                          cudaMemcpyDeviceToHost, k.stream));
+            SLCS_CUDA(cudaEventRecord(k.done, k.stream));
+            SLCS_CUDA(cudaStreamWaitEvent(st, k.done, 0));
+        }
+        SLCS_CUDA(cudaStreamSynchronize(st));
+        return slcs_device_status(P->device, 1);
+    }
     if (P->need_a) SLCS_CUDA(cudaMemcpyAsync(da, a, size_t(P->need_a), cudaMemcpyHostToDevice, st));
     if (P->need_b) SLCS_CUDA(cudaMemcpyAsync(db, b, size_t(P->need_b), cudaMemcpyHostToDevice, st));
     slcs_status s = slcs_batch_plan_run(P, da, db, dout, stream);
@@ -798,6 +922,12 @@ slcs_status slcs_batch_plan_run_host(slcs_batch_plan *P, const uint8_t *a, int64
 slcs_status slcs_batch_plan_destroy(slcs_batch_plan *P)
 {
     if (!P) return SLCS_OK;
+    for (auto &k : P->chunks) {
+        slcs_batch_plan_destroy(k.plan);
+        if (k.stream) cudaStreamDestroy(k.stream);
+        if (k.done) cudaEventDestroy(k.done);
+    }
+    if (P->chunk_start) cudaEventDestroy(P->chunk_start);
     if (P->gexec) cudaGraphExecDestroy(P->gexec);
     if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
     cudaFree(P->d_pairs);

@@ -343,3 +343,45 @@ def test_batch_default_plan_all_row_classes(cuda):
     got, info = _run_plan(batch, slcs.Config.make(), cuda)
     assert info["stream_classes"] >= 6 and info["wavefront_tasks"] > 0
     np.testing.assert_array_equal(got, _batch_expected(batch))
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_batch_run_host_chunked_golden(cuda, pinned):
+    """Host run of the 20,000-read batch (cut into chunks whose copies overlap
+    the combing of other chunks) against the oracle's digest, twice."""
+    import torch
+    g = _golden()["reads_20000"]
+    batch = W.reads_20000()
+    descs = slcs.pair_descs(batch)
+    _, total = batch.strand_offsets()
+    plan = slcs.BatchPlan(descs, slcs.Config.make(use_graph=1))
+    if pinned:
+        a = torch.from_numpy(batch.a_blob).pin_memory().numpy()
+        b = torch.from_numpy(batch.b_blob).pin_memory().numpy()
+        out = torch.empty(total, dtype=torch.int32).pin_memory().numpy()
+    else:
+        a, b, out = batch.a_blob, batch.b_blob, np.empty(total, np.int32)
+    for _ in range(2):
+        out[:] = -7
+        plan.run_host(a, b, out)
+        assert _sha256(out) == g["sha256_strands"]
+    plan.close()
+
+
+def test_batch_run_host_chunked_ragged(cuda):
+    """More than 8192 pairs with empty sides and odd offsets through the host
+    run, against the oracle."""
+    rng = np.random.default_rng(515)
+    pairs = []
+    for i in range(9001):
+        m = int(rng.integers(0, 300)) if i % 37 else 0
+        n = int(rng.integers(0, 400)) if i % 41 else 0
+        pairs.append((rng.integers(0, 4, m, dtype=np.uint8), rng.integers(0, 4, n, dtype=np.uint8)))
+    batch = _pack_unaligned(pairs, 515)
+    descs = slcs.pair_descs(batch)
+    _, total = batch.strand_offsets()
+    plan = slcs.BatchPlan(descs, slcs.Config.make())
+    out = np.full(total, -7, np.int32)
+    plan.run_host(batch.a_blob, batch.b_blob, out)
+    np.testing.assert_array_equal(out, _batch_expected(batch))
+    plan.close()
