@@ -473,7 +473,7 @@ slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_d
 // Chunks for host runs (an optimisation only: without them run_host copies
 // everything in, combs, and copies everything out).  Made for batches of at
 // least CHUNK_MIN_PAIRS pairs whose chunks' byte ranges do not overlap.
-static constexpr int HOST_CHUNKS = 4;
+static constexpr int HOST_CHUNKS = 8;
 static constexpr int32_t CHUNK_MIN_PAIRS = 8192;
 
 static void plan_add_chunks(slcs_batch_plan *P, const slcs_pair_desc *pairs, int32_t npairs, const slcs_config *cfg)
