@@ -558,14 +558,10 @@ __global__ void __launch_bounds__(256) glue_kernel(GlueArgs A)
         A.H[po + prow] = hi;
         A.R[po + pcol] = prow;
         A.HC[po + pcol] = hi;
+        A.res[po + prow] = pcol; // the union of both halves; the walk adds the fresh points
     }
 }
 
-__global__ void __launch_bounds__(256) union_kernel(const int32_t *C, int32_t *res, int k, const int32_t *bad)
-{
-    if (*bad) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) res[i] = C[i];
-}
 
 // ---------------------------------------------------------------------------
 // concurrent walk of large nodes
@@ -1219,8 +1215,7 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     int32_t *map_col = reinterpret_cast<int32_t *>(take(kk * 4));
     int32_t *bad = reinterpret_cast<int32_t *>(take(256));
     const size_t tints = table_ints(k, cutoff);
-    int32_t *tab_hi = reinterpret_cast<int32_t *>(take(tints * 4));
-    int32_t *tab_lo = reinterpret_cast<int32_t *>(take(tints * 4));
+    int32_t *tab_hi = reinterpret_cast<int32_t *>(take(2 * tints * 4)); // hi then lo counts of a level
     if (size_t(cur - static_cast<char *>(ws)) > ws_bytes) return fail(SLCS_ERR_ALLOC, "braid workspace too small");
 
     SLCS_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), st));
@@ -1279,14 +1274,14 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         GlueArgs G{res + kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1) + kk,
                    C, Rr, H, HC, res + kk * size_t(l), k, l, bad};
         glue_kernel<<<blocks_for(k, 256), 256, 0, st>>>(G);
-        union_kernel<<<blocks_for(k, 256), 256, 0, st>>>(C, res + kk * size_t(l), k, bad);
         int B, stride;
         walk_grid(k, l, B, stride);
         const int nodes = 1 << l;
-        const size_t tbytes = size_t(nodes) * stride * stride * 4;
-        SLCS_CUDA(cudaMemsetAsync(tab_hi, 0, tbytes, st));
-        SLCS_CUDA(cudaMemsetAsync(tab_lo, 0, tbytes, st));
-        TableArgs TA{C, H, tab_hi, tab_lo, k, l, B, stride, bad};
+        const size_t tentries = size_t(nodes) * stride * stride;
+        // hi and lo counts of the level side by side: one clear for both
+        int32_t *lvl_lo = tab_hi + tentries;
+        SLCS_CUDA(cudaMemsetAsync(tab_hi, 0, 2 * tentries * sizeof(int32_t), st));
+        TableArgs TA{C, H, tab_hi, lvl_lo, k, l, B, stride, bad};
         table_count_kernel<<<blocks_for(k, 256), 256, 0, st>>>(TA);
         const int rows = nodes * stride;
         table_rows_kernel<<<int((long(rows) * 32 + 255) / 256), 256, 0, st>>>(TA, nodes);
