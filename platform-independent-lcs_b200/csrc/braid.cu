@@ -16,16 +16,19 @@
 //   * A node at or below the cutoff is finished by one thread block: it loads
 //     the node into shared memory (16-bit local indices) and runs every lower
 //     level of its subtree there, down and back up, with block-wide scans.
-//   * Upward, a level first scatters both children's products into the
-//     parent's rows and columns (inverse_mapping, 191-202), then walks the ant
-//     (123-189) over every node, then writes the union of the two halves with
-//     the walk's fresh points on top (254-268).
+//   * Upward, a level scatters both children's products into the parent's
+//     rows and columns (inverse_mapping, 191-202) and, in the same pass, into
+//     the parent's result (the union of the two halves, 254-268); then it
+//     walks the ant (123-189) over every node, which writes the fresh points
+//     on top.
 //   * Walks of small nodes run one thread per node.  A large node's walk is cut
 //     into segments that run concurrently: on every diagonal e = col - row the
 //     walk sits one row above r*(e-1), the first point of diagonal e-1 where
 //     the dominance difference (hi points above-left minus lo points
 //     below-right) is non-negative, so a segment can start anywhere once r* is
-//     known there (see walk_segments).
+//     known there (walk_lanes_kernel: one lane per segment for short segments;
+//     walk_segments_kernel: one warp per segment with the rows and columns it
+//     can touch staged in shared memory).
 #include <climits>
 #include <cmath>
 #include <vector>
