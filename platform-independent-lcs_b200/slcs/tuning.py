@@ -65,7 +65,7 @@ def per_pair_loop(batch, a_d, b_d, out, stream_handle, limit=None):
 
 
 def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev, sampler=None):
-    """Plain per-pair loop, the 2^20 pair (best of 3 runs, with the SM clocks
+    """Plain per-pair loop, the 2^20 pair (best of 5 runs, with the SM clocks
     sampled while it runs when `sampler` -- a context-manager factory with a
     summary() -- is given), strips and braid products."""
     import torch
@@ -98,7 +98,7 @@ def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev, sampler=None):
     smp = sampler() if sampler else None
     if smp:
         smp.__enter__()
-    for _ in range(3):
+    for _ in range(5):
         e0.record(st)
         comb_pair(ad, bd, cfg=cfg, out=o)
         e1.record(st)
