@@ -460,36 +460,43 @@ struct NextCouple {
     NextPair<TM> A, B;
 };
 
-// Make a fetched couple current: packed row symbols and start ids.
+// Make a fetched couple current: packed row symbols and start ids.  This runs
+// on one lane at a time (each lane switches one step after its left
+// neighbour), so it is written to be short: per row one byte permute picks
+// both pairs' symbols, and the masks and start ids follow from the rows left
+// in each pair, m - r (the id + 1 of row r's h strand while r < m).
 template <int TM>
 __device__ __forceinline__ void take_couple(const CombLaunch &L, const NextCouple<TM> &N, int r0, CoupleTask<TM> &T,
                                             uint32_t (&ap)[TM], uint32_t (&hp)[TM])
 {
-    StreamTask<TM> A, B;
-    int aa[TM], ha[TM], ab[TM], hb[TM];
-    take_next<TM>(L, N.A, r0, A, aa, ha);
-    take_next<TM>(L, N.B, r0, B, ab, hb);
-    T.pa = A.pair;
-    T.pb = B.pair;
-    T.ma = A.m;
-    T.na = A.n;
-    T.mb = B.m;
-    T.nb_cols = B.n;
-    T.ba = A.b;
-    T.bb = B.b;
-    T.ha = A.h_out;
-    T.va = A.v_out;
-    T.hb = B.h_out;
-    T.vb = B.v_out;
-    T.nb = (max(A.n, B.n) + 3) / 4;
+    const bool va = N.A.pair >= 0, vb = N.B.pair >= 0;
+    T.pa = N.A.pair;
+    T.pb = N.B.pair;
+    T.ma = va ? N.A.d1.z : 0;
+    T.na = va ? N.A.d1.w : 0;
+    T.mb = vb ? N.B.d1.z : 0;
+    T.nb_cols = vb ? N.B.d1.w : 0;
+    const int64_t ba = va ? int64_t((uint64_t(uint32_t(N.A.d0.w)) << 32) | uint32_t(N.A.d0.z)) : 0;
+    const int64_t oa = va ? int64_t((uint64_t(uint32_t(N.A.d1.y)) << 32) | uint32_t(N.A.d1.x)) : 0;
+    const int64_t bb = vb ? int64_t((uint64_t(uint32_t(N.B.d0.w)) << 32) | uint32_t(N.B.d0.z)) : 0;
+    const int64_t ob = vb ? int64_t((uint64_t(uint32_t(N.B.d1.y)) << 32) | uint32_t(N.B.d1.x)) : 0;
+    T.ba = L.b_blob + ba;
+    T.bb = L.b_blob + bb;
+    T.ha = L.out + oa;
+    T.va = T.ha + T.ma;
+    T.hb = L.out + ob;
+    T.vb = T.hb + T.mb;
+    T.nb = (max(T.na, T.nb_cols) + 3) / 4;
+    const int ra = T.ma - r0, rb = T.mb - r0;
 #pragma unroll
     for (int k = 0; k < TM; ++k) {
-        const uint32_t lo = aa[k] < 0 ? 0x1FFu : uint32_t(aa[k]);
-        const uint32_t hi = ab[k] < 0 ? 0x1FFu : uint32_t(ab[k]);
-        ap[k] = lo | (hi << 16);
-        const uint32_t hl = ha[k] < 0 ? 0u : uint32_t(ha[k] + 1);
-        const uint32_t hh = hb[k] < 0 ? 0u : uint32_t(hb[k] + 1);
-        hp[k] = hl | (hh << 16);
+        const uint32_t j = uint32_t(k % 4);
+        // byte j of A's word to byte 0, byte j of B's word to byte 2
+        const uint32_t sym = __byte_perm(N.A.sym[k / 4], N.B.sym[k / 4], j | (j << 4) | ((4 + j) << 8) | ((4 + j) << 12)) &
+                             0x00FF00FFu;
+        const int hA = ra - k, hB = rb - k;
+        ap[k] = sym | (hA <= 0 ? 0x1FFu : 0u) | (hB <= 0 ? 0x1FF0000u : 0u);
+        hp[k] = uint32_t(max(hA, 0)) | (uint32_t(max(hB, 0)) << 16);
     }
 }
 
