@@ -69,6 +69,26 @@ int pick_tile_m(const slcs_config *cfg, int32_t m_typical, int64_t total_cells)
 {
     if (cfg && cfg->tile_m) return cfg->tile_m;
     (void)total_cells;
+    if (m_typical >= (1 << 19)) {
+        // All stripes of one long pair are resident at once and every warp
+        // stays on one SM sub-partition (4 per SM), so the busiest
+        // sub-partition sets the pace: pick the rows per lane that minimise
+        // its rows, ceil(stripes / sub-partitions) * rows per stripe (2^20
+        // rows: 14 -> 2341 stripes, 4 per sub-partition; 16 -> 2048 stripes,
+        // still 4 on most).  Ties go to the taller stripe.
+        const int64_t parts = 4 * int64_t(std::max(1, sm_count()));
+        int best = 16;
+        int64_t best_rows = INT64_MAX;
+        for (int tm : {16, 14, 12}) {
+            const int64_t stripes = stripes_of(m_typical, tm);
+            const int64_t rows = (stripes + parts - 1) / parts * tm;
+            if (rows < best_rows) {
+                best_rows = rows;
+                best = tm;
+            }
+        }
+        return best;
+    }
     if (m_typical >= 262144) return 16; // >= 512 stripes of 512 rows: enough warps in flight
     if (m_typical >= 65536) return 8;
     if (m_typical >= 8192) return 4;
@@ -97,8 +117,8 @@ int auto_strips(int32_t m, int32_t n)
     return S;
 }
 
-// 16 rows per lane leave room for 8 warps per block; the smaller tiles run 4.
-int pick_warps(const slcs_config *cfg, int tm) { return (cfg && cfg->warps) ? cfg->warps : (tm == 16 ? 8 : 4); }
+// 14 or 16 rows per lane leave room for 8 warps per block; the smaller tiles run 4.
+int pick_warps(const slcs_config *cfg, int tm) { return (cfg && cfg->warps) ? cfg->warps : (tm >= 14 ? 8 : 4); }
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -359,7 +379,7 @@ slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (m == 0 || n == 0) return write_identity(h_out, m, v_out, n, st);
     const int tm = pick_tile_m(cfg, m, int64_t(m) * n);
-    if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+    if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 14, 16");
     (void)sm_count(); // per-device set-up (memory pool) before the first allocation
     if (cfg && cfg->algo == SLCS_ALGO_STRIPS) return comb_strips(a, m, b, n, h_out, v_out, cfg, tm, pick_warps(cfg, tm), st);
     if (!cfg || (cfg->algo == SLCS_ALGO_AUTO && cfg->tile_m == 0 && cfg->warps == 0 && cfg->strips == 0)) {
@@ -579,7 +599,7 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
         P->tm = pick_tile_m(cfg, med, cells);
         if (!tile_m_supported(P->tm)) {
             delete P;
-            return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+            return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 14, 16");
         }
     } else {
         // Stream mode: pairs of at most 512 rows stream through segments,

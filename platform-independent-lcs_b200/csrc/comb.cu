@@ -40,10 +40,10 @@ namespace slcs {
 
 namespace {
 
-constexpr int TN = 4;      // columns per block (one 16-byte v vector)
+constexpr int TN = 4;      // columns per step of the stream kernels (one 16-byte v vector)
 constexpr int PREF = 4;    // blocks lane 0 prefetches ahead
 constexpr int RING = 8;    // shared-memory ring slots per warp (> PREF)
-constexpr int PUBLISH = 8; // blocks between progress releases
+constexpr int PUBLISH_COLS = 32; // columns between progress releases
 
 struct StripeWait {
     const int32_t *prog;
@@ -87,134 +87,197 @@ __device__ __forceinline__ void cell(int a_sym, int b_sym, int &h, int &v)
     h = nh;
 }
 
-template <int TM>
-__device__ __forceinline__ void comb_stripe(const CombLaunch &L, const PairDev &P, int64_t scr_off,
-                                            int stripe, int task, int4 *ring, int lane)
-{
-    const int m = P.m, n = P.n;
-    const uint8_t *__restrict__ a = L.a_blob + P.a_off;
-    const uint8_t *__restrict__ b = L.b_blob + P.b_off;
-    int32_t *hout = L.out + P.out_off;
-    int32_t *vout = hout + m;
-    int32_t *scr = L.scratch + scr_off;
+// One row stripe of one pair, combed by one warp.  TW columns form a block,
+// the unit of a step, of a scratch-row transfer and of the shuffle hand-off;
+// the ring holds RING blocks of TW strands per warp.  The kernels use TW = 4:
+// 8 columns per step passed the same parity tests but combed the 2^20 pair
+// about 20 % slower.
+template <int TM, int TW>
+struct Stripe {
+    static constexpr int Q = TW / 4;                 // int4 per block
+    static constexpr int PUBLISH = PUBLISH_COLS / TW; // blocks between releases
 
-    const int r0 = stripe * 32 * TM;
-    int av[TM], hv[TM];
+    const uint8_t *__restrict__ b;
+    int32_t *vout;
+    int32_t *scr;
+    int4 *ring;
+    int32_t *prog_mine;
+    StripeWait W;
+    int m, n, nb, lane;
+    bool first, has_next;
+    int av[TM], hv[TM], vc[TW];
+
+    // Column symbols of block blk (-2 past n).  FULL: the block is whole and
+    // b is aligned to the block's load width.
+    template <bool FULL>
+    __device__ __forceinline__ void symbols(int blk, bool act, int (&bs)[TW]) const
+    {
+        const int c = blk * TW;
+        if (FULL) {
+            if (TW == 8) {
+                const uint2 w = __ldg(reinterpret_cast<const uint2 *>(b + c));
 #pragma unroll
-    for (int k = 0; k < TM; ++k) {
-        const int r = r0 + lane * TM + k;
-        const bool in = r < m;
-        av[k] = in ? int(a[r]) : -1;
-        hv[k] = in ? (m - 1 - r) : INT_MIN;
-    }
-    const bool first = stripe == 0;
-    const bool has_next = r0 + 32 * TM < m;
-    const int nb = (n + TN - 1) / TN;
-    const bool b_aligned = (reinterpret_cast<uintptr_t>(b) & 3) == 0;
-
-    StripeWait W{L.progress + (task - 1), L.counters + 1, L.status, L.wait_ns, 0, 0, false};
-    int32_t *prog_mine = L.progress + task;
-
-    if (!first && lane == 0) {
-#pragma unroll
-        for (int d = 0; d < PREF; ++d) {
-            if (d < nb) {
-                W.until(d);
-                if (!W.dead) cp_async_cg16(&ring[d], scr + d * TN);
-            }
-            cp_async_commit();
-        }
-    }
-
-    int vc[TN];
-#pragma unroll
-    for (int j = 0; j < TN; ++j) vc[j] = INT_MAX;
-
-    const int steps = nb + 31;
-    for (int t = 0; t < steps; ++t) {
-        const int blk = t - lane;
-        const bool act = unsigned(blk) < unsigned(nb);
-
-        int vi[TN];
-#pragma unroll
-        for (int j = 0; j < TN; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1);
-
-        if (lane == 0) {
-            if (t < nb) {
-                const int c = t * TN;
-                if (first) {
-#pragma unroll
-                    for (int j = 0; j < TN; ++j) vi[j] = (c + j < n) ? m + c + j : INT_MAX;
-                } else {
-                    const int nxt = t + PREF;
-                    if (nxt < nb) {
-                        W.until(nxt);
-                        if (!W.dead) cp_async_cg16(&ring[nxt & (RING - 1)], scr + nxt * TN);
-                    }
-                    cp_async_commit();
-                    cp_async_wait<PREF>();
-                    const int4 x = ring[t & (RING - 1)];
-                    vi[0] = x.x;
-                    vi[1] = x.y;
-                    vi[2] = x.z;
-                    vi[3] = x.w;
-                    if (c + TN > n) {
-#pragma unroll
-                        for (int j = 0; j < TN; ++j)
-                            if (c + j >= n) vi[j] = INT_MAX;
-                    }
+                for (int j = 0; j < 4; ++j) {
+                    bs[j] = int((w.x >> (8 * j)) & 0xffu);
+                    bs[4 + j] = int((w.y >> (8 * j)) & 0xffu);
                 }
             } else {
-#pragma unroll
-                for (int j = 0; j < TN; ++j) vi[j] = INT_MAX;
-            }
-        }
-
-        int bs[TN];
-        if (act) {
-            const int c = blk * TN;
-            if (b_aligned && c + TN <= n) {
                 const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(b + c));
 #pragma unroll
-                for (int j = 0; j < TN; ++j) bs[j] = int((w >> (8 * j)) & 0xffu);
-            } else {
-#pragma unroll
-                for (int j = 0; j < TN; ++j) bs[j] = (c + j < n) ? int(__ldg(b + c + j)) : -2;
+                for (int j = 0; j < TW; ++j) bs[j] = int((w >> (8 * j)) & 0xffu);
             }
         } else {
 #pragma unroll
-            for (int j = 0; j < TN; ++j) bs[j] = -2;
+            for (int j = 0; j < TW; ++j) bs[j] = (act && c + j < n) ? int(__ldg(b + c + j)) : -2;
         }
+    }
 
+    // Lane 0: the v strands entering block t at the top of the stripe.
+    template <bool FULL>
+    __device__ __forceinline__ void top(int t, int (&vi)[TW])
+    {
+        const int c = t * TW;
+        if (!FULL && t >= nb) {
 #pragma unroll
-        for (int j = 0; j < TN; ++j) {
+            for (int j = 0; j < TW; ++j) vi[j] = INT_MAX;
+            return;
+        }
+        if (first) {
+#pragma unroll
+            for (int j = 0; j < TW; ++j) vi[j] = (FULL || c + j < n) ? m + c + j : INT_MAX;
+            return;
+        }
+        const int nxt = t + PREF;
+        if (nxt < nb) {
+            W.until(nxt);
+            if (!W.dead) {
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                    cp_async_cg16(&ring[(nxt & (RING - 1)) * Q + q], scr + nxt * TW + 4 * q);
+            }
+        }
+        cp_async_commit();
+        cp_async_wait<PREF>();
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int4 x = ring[(t & (RING - 1)) * Q + q];
+            vi[4 * q + 0] = x.x;
+            vi[4 * q + 1] = x.y;
+            vi[4 * q + 2] = x.z;
+            vi[4 * q + 3] = x.w;
+        }
+        // Past n the producer's strands are INT_MAX already (masked columns
+        // never swap), so a partial last block needs no mask here.
+    }
+
+    // Step t: lane l combs block t - l.  FULL: every lane's block is whole
+    // and lies in [0, nb), and the symbols of b can be loaded as words.
+    template <bool FULL>
+    __device__ __forceinline__ void step(int t)
+    {
+        const int blk = t - lane;
+        const bool act = FULL || unsigned(blk) < unsigned(nb);
+        int vi[TW];
+#pragma unroll
+        for (int j = 0; j < TW; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1);
+        if (lane == 0) top<FULL>(t, vi);
+        int bs[TW];
+        symbols<FULL>(blk, act, bs);
+#pragma unroll
+        for (int j = 0; j < TW; ++j) {
             int v = vi[j];
 #pragma unroll
             for (int k = 0; k < TM; ++k) cell(av[k], bs[j], hv[k], v);
             vc[j] = v;
         }
-
         if (lane == 31 && act) {
-            const int c = blk * TN;
+            const int c = blk * TW;
             if (has_next) {
-                *reinterpret_cast<int4 *>(scr + c) = make_int4(vc[0], vc[1], vc[2], vc[3]);
-                if ((blk & (PUBLISH - 1)) == PUBLISH - 1 || blk == nb - 1) st_release_gpu(prog_mine, blk + 1);
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                    *reinterpret_cast<int4 *>(scr + c + 4 * q) =
+                        make_int4(vc[4 * q], vc[4 * q + 1], vc[4 * q + 2], vc[4 * q + 3]);
+                if ((blk & (PUBLISH - 1)) == PUBLISH - 1 || (!FULL && blk == nb - 1))
+                    st_release_gpu(prog_mine, blk + 1);
             } else {
 #pragma unroll
-                for (int j = 0; j < TN; ++j)
-                    if (c + j < n) vout[c + j] = vc[j];
+                for (int j = 0; j < TW; ++j)
+                    if (FULL || c + j < n) vout[c + j] = vc[j];
             }
         }
     }
-    if (!first && lane == 0) cp_async_wait<0>();
+};
+
+template <int TM, int TW = 4>
+__device__ __forceinline__ void comb_stripe(const CombLaunch &L, const PairDev &P, int64_t scr_off,
+                                            int stripe, int task, int4 *ring, int lane)
+{
+    Stripe<TM, TW> S;
+    const int m = P.m, n = P.n;
+    const uint8_t *__restrict__ a = L.a_blob + P.a_off;
+    int32_t *hout = L.out + P.out_off;
+    S.b = L.b_blob + P.b_off;
+    S.vout = hout + m;
+    S.scr = L.scratch + scr_off;
+    S.ring = ring;
+    S.prog_mine = L.progress + task;
+    S.W = StripeWait{L.progress + (task - 1), L.counters + 1, L.status, L.wait_ns, 0, 0, false};
+    S.m = m;
+    S.n = n;
+    S.nb = (n + TW - 1) / TW;
+    S.lane = lane;
+
+    const int r0 = stripe * 32 * TM;
+#pragma unroll
+    for (int k = 0; k < TM; ++k) {
+        const int r = r0 + lane * TM + k;
+        const bool in = r < m;
+        S.av[k] = in ? int(a[r]) : -1;
+        S.hv[k] = in ? (m - 1 - r) : INT_MIN;
+    }
+    S.first = stripe == 0;
+    S.has_next = r0 + 32 * TM < m;
+    const int nb = S.nb;
+
+    if (!S.first && lane == 0) {
+#pragma unroll
+        for (int d = 0; d < PREF; ++d) {
+            if (d < nb) {
+                S.W.until(d);
+                if (!S.W.dead) {
+#pragma unroll
+                    for (int q = 0; q < Stripe<TM, TW>::Q; ++q)
+                        cp_async_cg16(&ring[d * Stripe<TM, TW>::Q + q], S.scr + d * TW + 4 * q);
+                }
+            }
+            cp_async_commit();
+        }
+    }
+
+#pragma unroll
+    for (int j = 0; j < TW; ++j) S.vc[j] = INT_MAX;
+
+    // Steps 0..30 fill the pipeline and the last 32 drain it (some lanes idle,
+    // the last block may be partial); in between every lane combs a whole
+    // block, so those steps run without bounds checks.
+    const bool b_aligned = (reinterpret_cast<uintptr_t>(S.b) & (TW - 1)) == 0;
+    const int fill = nb + 31 < 31 ? nb + 31 : 31;
+    const int full_end = (b_aligned && nb - 1 > 31) ? nb - 1 : fill;
+    int t = 0;
+    for (; t < fill; ++t) S.template step<false>(t);
+    for (; t < full_end; ++t) S.template step<true>(t);
+    for (; t < nb + 31; ++t) S.template step<false>(t);
+    if (!S.first && lane == 0) cp_async_wait<0>();
 
 #pragma unroll
     for (int k = 0; k < TM; ++k) {
         const int r = r0 + lane * TM + k;
-        if (r < m) hout[m - 1 - r] = hv[k];
+        if (r < m) hout[m - 1 - r] = S.hv[k];
     }
 }
 
+// WARPS is the largest block the kernel is launched with (the ring is sized
+// for it); a launch may use fewer warps per block.
 template <int TM, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) comb_wavefront_kernel(const CombLaunch L)
 {
@@ -663,9 +726,76 @@ __global__ void strands_to_perm_kernel(const int32_t *__restrict__ h, int32_t m,
     }
 }
 
+// Balanced launch: when every stripe can be resident at once, each SM gets
+// one block of ceil(stripes / SMs) warps, so no SM hosts more stripes than
+// another by more than one.  (With several blocks per SM, tickets went to
+// whichever warps started first, and an SM holding 16 stripes instead of the
+// average 13.8 set the pace of the whole wavefront.)  Dynamic shared memory of
+// more than half an SM keeps a second block off every SM.
+constexpr int WF_SM_WARPS = 16;
+
+template <int TM>
+struct Balanced {
+    bool ok = false;
+    int smem = 0;
+};
+
+template <int TM>
+slcs_status balanced_setup(Balanced<TM> &B)
+{
+    int dev = 0, per_sm = 0, optin = 0;
+    SLCS_CUDA(cudaGetDevice(&dev));
+    SLCS_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    SLCS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa{};
+    SLCS_CUDA(cudaFuncGetAttributes(&fa, comb_wavefront_kernel<TM, WF_SM_WARPS>));
+    const int want = per_sm / 2 + 1024 - int(fa.sharedSizeBytes);
+    if (want <= 0 || want + int(fa.sharedSizeBytes) > optin) return SLCS_OK;
+    SLCS_CUDA(cudaFuncSetAttribute(comb_wavefront_kernel<TM, WF_SM_WARPS>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, want));
+    int occ = 0;
+    SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WF_SM_WARPS>,
+                                                            WF_SM_WARPS * 32, size_t(want)));
+    B.smem = want;
+    B.ok = occ == 1;
+    return SLCS_OK;
+}
+
+// Launches the balanced form when it applies; *done tells whether it did.
+template <int TM>
+slcs_status launch_balanced(const CombLaunch &L, long sms, cudaStream_t stream, int *grid_out, bool *done)
+{
+    static Balanced<TM> B;
+    static int state = -1;
+    static std::mutex mu;
+    *done = false;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (state < 0) {
+            const slcs_status s = balanced_setup(B);
+            if (s != SLCS_OK) return s;
+            state = 1;
+        }
+    }
+    if (!B.ok || sms < 1) return SLCS_OK;
+    const long per_sm = (long(L.ntasks) + sms - 1) / sms;
+    if (per_sm > WF_SM_WARPS) return SLCS_OK;
+    *done = true;
+    if (stream == PREPARE_ONLY) return SLCS_OK;
+    const long grid = std::min<long>(sms, L.ntasks);
+    comb_wavefront_kernel<TM, WF_SM_WARPS><<<int(grid), int(per_sm) * 32, size_t(B.smem), stream>>>(L);
+    if (grid_out) *grid_out = int(grid);
+    SLCS_CUDA(cudaGetLastError());
+    return SLCS_OK;
+}
+
 template <int TM, int WARPS>
 slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_out)
 {
+    const long sms = sm_count();
+    bool done = false;
+    const slcs_status bs = launch_balanced<TM>(L, sms, stream, grid_out, &done);
+    if (bs != SLCS_OK || done) return bs;
     static int occ = -1;
     static std::mutex mu;
     {
@@ -677,12 +807,10 @@ slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_o
         }
     }
     if (stream == PREPARE_ONLY) return SLCS_OK;
-    // One warp per stripe at most; beyond one block per SM the grid is rounded
-    // up to a multiple of the SM count (surplus warps find no ticket and
-    // exit), so that every SM hosts the same number of warps.  With 2048
-    // stripes of 8-warp blocks, 256 blocks left 40 SMs at half load and the
-    // stripes on the full SMs set the pace of the whole wavefront.
-    const long sms = sm_count();
+    // More stripes than fit at once: persistent blocks take stripes from the
+    // ticket counter.  Beyond one block per SM the grid is rounded up to a
+    // multiple of the SM count, so that every SM hosts the same number of
+    // warps.
     long want = (long(L.ntasks) + WARPS - 1) / WARPS;
     if (want > sms) want = (want + sms - 1) / sms * sms;
     long grid = sms * occ;
@@ -724,6 +852,9 @@ slcs_status launch_batch_variant(const BatchLaunch &B, cudaStream_t stream, int 
 template <int TM, int WARPS>
 slcs_status launch_variant_on(const CombLaunch &L, int sms, cudaStream_t stream)
 {
+    bool done = false;
+    const slcs_status bs = launch_balanced<TM>(L, sms, stream, nullptr, &done);
+    if (bs != SLCS_OK || done) return bs;
     static int occ = -1;
     static std::mutex mu;
     {
@@ -758,9 +889,10 @@ slcs_status launch_comb_on(const CombLaunch &L, int tile_m, int warps, int sms, 
         SLCS_TM_ON(4)
         SLCS_TM_ON(8)
         SLCS_TM_ON(12)
+        SLCS_TM_ON(14)
         SLCS_TM_ON(16)
     default:
-        return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+        return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 14, 16");
     }
 #undef SLCS_TM_ON
 }
@@ -780,7 +912,7 @@ slcs_status launch_batch(const BatchLaunch &B, int tns, cudaStream_t stream, int
     return fail(SLCS_ERR_UNSUPPORTED, "stream columns per step must be 4 or 8");
 }
 
-bool tile_m_supported(int tm) { return tm == 2 || tm == 4 || tm == 8 || tm == 12 || tm == 16; }
+bool tile_m_supported(int tm) { return tm == 2 || tm == 4 || tm == 8 || tm == 12 || tm == 14 || tm == 16; }
 int rows_per_stripe(int tm) { return 32 * tm; }
 
 slcs_status launch_comb(const CombLaunch &L, int tile_m, int warps, cudaStream_t stream, int *grid_out)
@@ -796,9 +928,10 @@ slcs_status launch_comb(const CombLaunch &L, int tile_m, int warps, cudaStream_t
         SLCS_TM_CASE(4)
         SLCS_TM_CASE(8)
         SLCS_TM_CASE(12)
+        SLCS_TM_CASE(14)
         SLCS_TM_CASE(16)
     default:
-        return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+        return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 14, 16");
     }
 #undef SLCS_TM_CASE
 }

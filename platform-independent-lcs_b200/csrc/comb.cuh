@@ -56,7 +56,7 @@ inline int32_t stripes_of(int32_t m, int tm) { return m <= 0 ? 0 : (m + 32 * tm 
 // Scratch elements a pair needs (0 when it has a single stripe).
 inline int64_t scratch_elems(int32_t m, int32_t n, int tm)
 {
-    return stripes_of(m, tm) > 1 ? (int64_t(n) + 3) / 4 * 4 : 0;
+    return stripes_of(m, tm) > 1 ? (int64_t(n) + 7) / 8 * 8 : 0;
 }
 
 // Passed as the stream, makes a launch function only do its one-time set-up

@@ -89,7 +89,7 @@ extern "C" SLCS_API slcs_status slcs_comb_pair_noalloc(const uint8_t *a, int32_t
         return SLCS_OK;
     }
     const int tm = noalloc_tile_m(cfg, m);
-    if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 16");
+    if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 14, 16");
     const int32_t ntasks = stripes_of(m, tm);
     // [counters(4) | progress(ntasks)] rounded to 256 bytes, then the
     // 16-byte aligned strand row the stripes hand down.

@@ -28,7 +28,7 @@ SHAPES = [(1, 1), (1, 7), (7, 1), (2, 3), (31, 33), (32, 32), (33, 4), (64, 129)
           (257, 100), (500, 3), (3, 500), (1000, 1001), (1023, 517), (2049, 2047)]
 
 
-@pytest.mark.parametrize("tm", [2, 4, 8, 12, 16])
+@pytest.mark.parametrize("tm", [2, 4, 8, 12, 14, 16])
 def test_pair_shapes(cuda, tm):
     rng = np.random.default_rng(10 + tm)
     for (m, n) in SHAPES:
@@ -36,6 +36,18 @@ def test_pair_shapes(cuda, tm):
         a = rng.integers(0, sigma, m, dtype=np.uint8)
         b = rng.integers(0, sigma, n, dtype=np.uint8)
         _check_pair(a, b, cuda, slcs.Config.make(tile_m=tm))
+
+
+@pytest.mark.parametrize("tm,m,n", [(2, 160000, 333), (14, 7 * 448 + 5, 1001), (16, 64 * 512 + 1, 97)])
+def test_pair_stripe_counts(cuda, tm, m, n):
+    """Stripe counts around the resident capacity: 2500 stripes of 64 rows are
+    more than one launch holds at once (persistent blocks take stripes from the
+    ticket counter); the others run one block per SM, the last one with a
+    single-row stripe at the bottom."""
+    rng = np.random.default_rng(m + n)
+    a = rng.integers(0, 4, m, dtype=np.uint8)
+    b = rng.integers(0, 4, n, dtype=np.uint8)
+    _check_pair(a, b, cuda, slcs.Config.make(tile_m=tm))
 
 
 @pytest.mark.parametrize("warps", [2, 4, 8])
