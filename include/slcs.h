@@ -51,7 +51,7 @@ typedef enum {
 enum {
     SLCS_ALGO_AUTO = 0,      /* let the engine choose (cost model, else heuristic)     */
     SLCS_ALGO_WAVEFRONT = 1, /* row stripes on warps, strands handed down through HBM */
-    SLCS_ALGO_STRIPS = 2     /* column strips combed independently, then braid-merged */
+    SLCS_ALGO_STRIPS = 2     /* tiles (column strips x row bands) combed independently, then braid-merged */
 };
 
 /* Tuning knobs.  Zero in any field means "engine default". */
@@ -68,7 +68,8 @@ typedef struct {
     int32_t blocks_per_sm; /* batch plans: resident blocks per SM (default: occupancy) */
     int32_t strand_bits;   /* batch plans: 16 = combine two pairs per register where ids fit 15 bits,
                               32 = 32-bit strands only, 0 = engine default                 */
-    int32_t reserved[5];
+    int32_t bands;         /* row bands of a for SLCS_ALGO_STRIPS (glued by row-glue products) */
+    int32_t reserved[4];
 } slcs_config;
 
 /* One pair of a batch: symbols at a_blob[a_offset .. +m) and b_blob[b_offset .. +n);
@@ -106,6 +107,24 @@ SLCS_API slcs_status slcs_device_name(int32_t device, char *buf, int32_t len);
  * fixup (src/lcs_grid.hpp:451-493): every cell is combed on the device. */
 SLCS_API slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n,
                            int32_t *h_out, int32_t *v_out, const slcs_config *cfg, void *stream);
+
+/* How slcs_comb_pair combs an m x n pair under cfg: the kernel family
+ * (SLCS_ALGO_WAVEFRONT, or SLCS_ALGO_STRIPS for band x strip tiles merged by
+ * braid products), rows per lane, warps per block, the tiling and the number
+ * of row stripes.  No counterpart in the reference, whose procedures are
+ * chosen by name (src/algorithm_registry.cpp:149-163).  Needs a device (it
+ * reads the SM count) but launches nothing. */
+typedef struct {
+    int32_t algo;         /* SLCS_ALGO_WAVEFRONT or SLCS_ALGO_STRIPS                  */
+    int32_t tile_m;       /* rows of a per lane                                      */
+    int32_t warps;        /* warps per block (when stripes outnumber the SM slots)   */
+    int32_t strips;       /* column strips of b                                      */
+    int32_t bands;        /* row bands of a                                          */
+    int32_t braid_cutoff; /* steady-ant cutoff of the merge products (0: no merge)   */
+    int32_t stripes;      /* row stripes of all tiles (warp tasks of the comb)       */
+    int32_t reserved[9];
+} slcs_pair_info;
+SLCS_API slcs_status slcs_pair_plan_info(int32_t m, int32_t n, const slcs_config *cfg, slcs_pair_info *info);
 
 /* One pair, device pointers, without allocating anything.  No counterpart in
  * the reference; it exists for callers that cannot allocate device memory at

@@ -117,8 +117,75 @@ int auto_strips(int32_t m, int32_t n)
     return S;
 }
 
+// Row bands for one tall pair (at least 2^19 rows) when nothing is
+// configured.  The stripes of a band form a chain that fills and drains in
+// about 44 steps of 4 columns per stripe, so a pair combed in R bands spends
+// about (n + 176 * stripes / R) / n times its cell time; every band adds
+// row-glue products, about log2(R) * m + (R - 1) * n permutation entries in
+// all.  The constants (3.5 Tcells/s, 1.5 ns per entry) are fitted to B200
+// timings of the 2^20 x 2^20 pair (R = 1, 2, 4, 8, 16: 410, 348, 327, 324,
+// 334 ms).
+int auto_bands(int32_t m, int32_t n, int tm)
+{
+    if (m < (1 << 19) || n <= 0) return 1;
+    const double stripes = double(stripes_of(m, tm));
+    const double cells = double(m) * double(n);
+    int best = 1;
+    double best_t = 0;
+    for (int R = 1; R <= 16 && R <= stripes; R *= 2) {
+        const double fill = (double(n) + 176.0 * std::ceil(stripes / R)) / double(n);
+        const double t = cells / 3.5e12 * fill + 1.5e-9 * (std::log2(double(R)) * m + double(R - 1) * n);
+        if (R == 1 || t < best_t) {
+            best = R;
+            best_t = t;
+        }
+    }
+    return best;
+}
+
 // 14 or 16 rows per lane leave room for 8 warps per block; the smaller tiles run 4.
 int pick_warps(const slcs_config *cfg, int tm) { return (cfg && cfg->warps) ? cfg->warps : (tm >= 14 ? 8 : 4); }
+
+// How slcs_comb_pair combs one pair: the effective configuration (algo
+// WAVEFRONT or STRIPS with tile_m, warps, strips, bands, braid_cutoff set).
+struct PairPlan {
+    slcs_config c;
+};
+
+slcs_status plan_pair(int32_t m, int32_t n, const slcs_config *cfg, PairPlan *P)
+{
+    P->c = cfg ? *cfg : slcs_config{};
+    slcs_config &c = P->c;
+    const int tm = pick_tile_m(cfg, m, int64_t(m) * n);
+    if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 14, 16");
+    const bool auto_all = !cfg || (cfg->algo == SLCS_ALGO_AUTO && cfg->tile_m == 0 && cfg->warps == 0 &&
+                                   cfg->strips == 0 && cfg->bands == 0);
+    c.tile_m = tm;
+    c.warps = pick_warps(cfg, tm);
+    if (c.algo == SLCS_ALGO_STRIPS) {
+        c.strips = strip_count(cfg, n);
+        c.bands = band_count(cfg, m, tm);
+        if (c.braid_cutoff <= 0) c.braid_cutoff = 1024;
+        return SLCS_OK;
+    }
+    c.algo = SLCS_ALGO_WAVEFRONT;
+    c.strips = 1;
+    c.bands = 1;
+    if (!auto_all) return SLCS_OK;
+    const int R = auto_bands(m, n, tm);
+    const int S = R > 1 ? 1 : auto_strips(m, n);
+    if (R > 1 || S > 1) {
+        c.algo = SLCS_ALGO_STRIPS;
+        c.strips = S;
+        c.bands = R;
+        if (S > 1) { // short pairs: column strips of 16-row stripes, 4 warps per block
+            c.tile_m = 16;
+            c.warps = 4;
+        }
+        if (c.braid_cutoff <= 0) c.braid_cutoff = 256;
+    }
+    return SLCS_OK;
+}
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -378,22 +445,12 @@ slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_
     if (int64_t(m) + n > INT32_MAX) return fail(SLCS_ERR_RANGE, "m+n exceeds int32 strand ids");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (m == 0 || n == 0) return write_identity(h_out, m, v_out, n, st);
-    const int tm = pick_tile_m(cfg, m, int64_t(m) * n);
-    if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 14, 16");
     (void)sm_count(); // per-device set-up (memory pool) before the first allocation
-    if (cfg && cfg->algo == SLCS_ALGO_STRIPS) return comb_strips(a, m, b, n, h_out, v_out, cfg, tm, pick_warps(cfg, tm), st);
-    if (!cfg || (cfg->algo == SLCS_ALGO_AUTO && cfg->tile_m == 0 && cfg->warps == 0 && cfg->strips == 0)) {
-        const int S = auto_strips(m, n);
-        if (S > 1) {
-            slcs_config c = cfg ? *cfg : slcs_config{};
-            c.algo = SLCS_ALGO_STRIPS;
-            c.strips = S;
-            c.tile_m = 16;
-            c.warps = 4;
-            if (c.braid_cutoff <= 0) c.braid_cutoff = 256;
-            return comb_strips(a, m, b, n, h_out, v_out, &c, 16, 4, st);
-        }
-    }
+    PairPlan pp;
+    const slcs_status ps = plan_pair(m, n, cfg, &pp);
+    if (ps != SLCS_OK) return ps;
+    const int tm = pp.c.tile_m;
+    if (pp.c.algo == SLCS_ALGO_STRIPS) return comb_strips(a, m, b, n, h_out, v_out, &pp.c, tm, pp.c.warps, st);
     const int32_t ntasks = stripes_of(m, tm);
     const size_t work_bytes = align_up(sizeof(int32_t) * (4 + size_t(ntasks)), 256);
     const size_t scr_bytes = sizeof(int32_t) * size_t(scratch_elems(m, n, tm));
@@ -422,13 +479,13 @@ slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_
     L.single.out_off = 0;
     slcs_status s;
     if (v_out == h_out + m) {
-        s = launch_comb(L, tm, pick_warps(cfg, tm), st, nullptr);
+        s = launch_comb(L, tm, pp.c.warps, st, nullptr);
     } else {
         // Comb into a contiguous temporary, then copy v out.
         int32_t *tmp = nullptr;
         SLCS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&tmp), sizeof(int32_t) * (size_t(m) + n), st));
         L.out = tmp;
-        s = launch_comb(L, tm, pick_warps(cfg, tm), st, nullptr);
+        s = launch_comb(L, tm, pp.c.warps, st, nullptr);
         if (s == SLCS_OK) {
             SLCS_CUDA(cudaMemcpyAsync(h_out, tmp, sizeof(int32_t) * m, cudaMemcpyDeviceToDevice, st));
             SLCS_CUDA(cudaMemcpyAsync(v_out, tmp + m, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st));
@@ -824,6 +881,26 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
         return cuda_fail(e, "batch plan upload");
     }
     *plan_out = P;
+    return SLCS_OK;
+}
+
+slcs_status slcs_pair_plan_info(int32_t m, int32_t n, const slcs_config *cfg, slcs_pair_info *info)
+{
+    if (!info) return fail(SLCS_ERR_INVALID, "null info");
+    if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
+    *info = slcs_pair_info{};
+    if (m == 0 || n == 0) return SLCS_OK;
+    (void)sm_count();
+    PairPlan pp;
+    const slcs_status s = plan_pair(m, n, cfg, &pp);
+    if (s != SLCS_OK) return s;
+    info->algo = pp.c.algo;
+    info->tile_m = pp.c.tile_m;
+    info->warps = pp.c.warps;
+    info->strips = pp.c.strips;
+    info->bands = pp.c.bands;
+    info->braid_cutoff = pp.c.algo == SLCS_ALGO_STRIPS ? pp.c.braid_cutoff : 0;
+    info->stripes = stripes_of(m, pp.c.tile_m) * (pp.c.algo == SLCS_ALGO_STRIPS ? pp.c.strips : 1);
     return SLCS_OK;
 }
 

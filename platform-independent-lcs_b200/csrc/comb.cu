@@ -33,6 +33,7 @@
 //     fixup.
 #include <climits>
 #include <mutex>
+#include <type_traits>
 
 #include "comb.cuh"
 
@@ -107,29 +108,29 @@ struct Stripe {
     bool first, has_next;
     int av[TM], hv[TM], vc[TW];
 
-    // Column symbols of block blk (-2 past n).  FULL: the block is whole and
-    // b is aligned to the block's load width.
-    template <bool FULL>
+    // Column symbols of a whole block as one word (b aligned to its size).
+    using Word = typename std::conditional<TW == 8, uint2, uint32_t>::type;
+    Word bnext; // the word of the block this lane combs next (main loop)
+
+    __device__ __forceinline__ Word word(int blk) const { return __ldg(reinterpret_cast<const Word *>(b + blk * TW)); }
+
+    __device__ __forceinline__ static void unpack(uint32_t w, int *bs)
+    {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bs[j] = int((w >> (8 * j)) & 0xffu);
+    }
+    __device__ __forceinline__ static void unpack(uint2 w, int *bs)
+    {
+        unpack(w.x, bs);
+        unpack(w.y, bs + 4);
+    }
+
+    // Column symbols of block blk: -2 past n or when the lane is idle.
     __device__ __forceinline__ void symbols(int blk, bool act, int (&bs)[TW]) const
     {
         const int c = blk * TW;
-        if (FULL) {
-            if (TW == 8) {
-                const uint2 w = __ldg(reinterpret_cast<const uint2 *>(b + c));
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    bs[j] = int((w.x >> (8 * j)) & 0xffu);
-                    bs[4 + j] = int((w.y >> (8 * j)) & 0xffu);
-                }
-            } else {
-                const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(b + c));
-#pragma unroll
-                for (int j = 0; j < TW; ++j) bs[j] = int((w >> (8 * j)) & 0xffu);
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < TW; ++j) bs[j] = (act && c + j < n) ? int(__ldg(b + c + j)) : -2;
-        }
+        for (int j = 0; j < TW; ++j) bs[j] = (act && c + j < n) ? int(__ldg(b + c + j)) : -2;
     }
 
     // Lane 0: the v strands entering block t at the top of the stripe.
@@ -182,7 +183,14 @@ struct Stripe {
         for (int j = 0; j < TW; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1);
         if (lane == 0) top<FULL>(t, vi);
         int bs[TW];
-        symbols<FULL>(blk, act, bs);
+        if (FULL) {
+            // The word was loaded one step ago; fetch the next one now, so
+            // that the load's latency hides behind this step's cells.
+            unpack(bnext, bs);
+            bnext = word(blk + 1);
+        } else {
+            symbols(blk, act, bs);
+        }
 #pragma unroll
         for (int j = 0; j < TW; ++j) {
             int v = vi[j];
@@ -257,12 +265,14 @@ __device__ __forceinline__ void comb_stripe(const CombLaunch &L, const PairDev &
 #pragma unroll
     for (int j = 0; j < TW; ++j) S.vc[j] = INT_MAX;
 
-    // Steps 0..30 fill the pipeline and the last 32 drain it (some lanes idle,
+    // Steps 0..30 fill the pipeline and the last 33 drain it (some lanes idle,
     // the last block may be partial); in between every lane combs a whole
-    // block, so those steps run without bounds checks.
+    // block, and the block after it is whole too (its symbols are loaded one
+    // step ahead), so those steps run without bounds checks.
     const bool b_aligned = (reinterpret_cast<uintptr_t>(S.b) & (TW - 1)) == 0;
     const int fill = nb + 31 < 31 ? nb + 31 : 31;
-    const int full_end = (b_aligned && nb - 1 > 31) ? nb - 1 : fill;
+    const int full_end = (b_aligned && nb - 2 > 31) ? nb - 2 : fill;
+    if (full_end > fill) S.bnext = S.word(fill - lane);
     int t = 0;
     for (; t < fill; ++t) S.template step<false>(t);
     for (; t < full_end; ++t) S.template step<true>(t);
@@ -276,31 +286,44 @@ __device__ __forceinline__ void comb_stripe(const CombLaunch &L, const PairDev &
     }
 }
 
+// Task k of the launch: its pair, stripe and scratch offset.
+__device__ __forceinline__ void task_of(const CombLaunch &L, int k, PairDev &P, int &stripe, int64_t &so)
+{
+    if (L.tasks) {
+        const int2 tk = L.tasks[k];
+        P = L.pairs[tk.x];
+        stripe = tk.y;
+        so = L.scratch_off[tk.x];
+    } else {
+        P = L.single;
+        stripe = k;
+        so = 0;
+    }
+}
+
 // WARPS is the largest block the kernel is launched with (the ring is sized
-// for it); a launch may use fewer warps per block.
+// for it); a launch may use fewer warps per block.  Warps take tasks from the
+// ticket counter: a task's producer always holds a smaller ticket, so it was
+// claimed by a warp that is already running, whatever the number of blocks
+// the GPU holds at once.  (A static map, warp w of block b on task
+// w * gridDim.x + b in a cooperative launch, spreads consecutive stripes over
+// the SMs; it combed the 2^20 pair in 763 ms instead of 407 ms, because the
+// four stripes sharing a sub-partition then start and finish far apart.)
 template <int TM, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) comb_wavefront_kernel(const CombLaunch L)
 {
     __shared__ __align__(16) int4 ring[WARPS][RING];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
+    PairDev P;
+    int stripe;
+    int64_t so;
     for (;;) {
         int k = 0;
         if (lane == 0) k = ld_relaxed_gpu(L.counters + 1) ? INT_MAX : atomicAdd(L.counters, 1);
         k = __shfl_sync(FULL_MASK, k, 0);
         if (k >= L.ntasks) break;
-        PairDev P;
-        int stripe;
-        int64_t so = 0;
-        if (L.tasks) {
-            const int2 tk = L.tasks[k];
-            P = L.pairs[tk.x];
-            stripe = tk.y;
-            so = L.scratch_off[tk.x];
-        } else {
-            P = L.single;
-            stripe = k;
-        }
+        task_of(L, k, P, stripe, so);
         comb_stripe<TM>(L, P, so, stripe, k, ring[w], lane);
     }
 }
@@ -734,14 +757,13 @@ __global__ void strands_to_perm_kernel(const int32_t *__restrict__ h, int32_t m,
 // more than half an SM keeps a second block off every SM.
 constexpr int WF_SM_WARPS = 16;
 
-template <int TM>
 struct Balanced {
     bool ok = false;
     int smem = 0;
 };
 
 template <int TM>
-slcs_status balanced_setup(Balanced<TM> &B)
+slcs_status balanced_setup(Balanced &B)
 {
     int dev = 0, per_sm = 0, optin = 0;
     SLCS_CUDA(cudaGetDevice(&dev));
@@ -765,14 +787,14 @@ slcs_status balanced_setup(Balanced<TM> &B)
 template <int TM>
 slcs_status launch_balanced(const CombLaunch &L, long sms, cudaStream_t stream, int *grid_out, bool *done)
 {
-    static Balanced<TM> B;
+    static Balanced B;
     static int state = -1;
     static std::mutex mu;
     *done = false;
     {
         std::lock_guard<std::mutex> g(mu);
         if (state < 0) {
-            const slcs_status s = balanced_setup(B);
+            const slcs_status s = balanced_setup<TM>(B);
             if (s != SLCS_OK) return s;
             state = 1;
         }

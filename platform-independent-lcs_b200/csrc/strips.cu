@@ -1,17 +1,22 @@
-// strips.cu -- one pair combed as column strips, then merged by braid
-// multiplication.
+// strips.cu -- one pair combed as tiles, then merged by braid multiplication.
 //
-// b is cut into S column strips b_1..b_S.  Every strip pair (a, b_s) is an
-// independent comb (one persistent wavefront launch over all strips), its
-// strands become the permutation P(a, b_s) (src/permutation_matrix.hpp:88-115),
-// and a balanced tree of sticky-braid products with overlap k = m glues them:
-// staggered_multiply<false>(P(a, x), P(a, y), m) == P(a, x y)
-// (src/braid_multiplication.hpp:273-407).  The last product is turned back
-// into strands, so the caller sees exactly what the direct comb returns.
+// a is cut into R row bands a_1..a_R and b into S column strips b_1..b_S.
+// Every tile (a_r, b_s) is an independent comb (one persistent wavefront
+// launch over all tiles), its strands become the permutation P(a_r, b_s)
+// (src/permutation_matrix.hpp:88-115), and balanced trees of sticky-braid
+// products glue them (src/braid_multiplication.hpp:273-407):
+//   staggered_multiply<false>(P(a_r, x), P(a_r, y), |a_r|) == P(a_r, x y)
+//   staggered_multiply<true>(P(x, b), P(y, b), |b|)       == P(x y, b)
+// first the strips of every band, then the bands.  The last product is turned
+// back into strands, so the caller sees exactly what the direct comb returns.
 //
 // This is the reference's tiled decomposition (tiles combed apart, then their
-// permutations multiplied) at strip granularity; it is also the per-GPU unit
-// of the multi-GPU split, where each rank combs one strip.
+// permutations multiplied) at a coarse granularity.  Why it pays on the GPU:
+// the stripes of one tile form a chain (stripe t starts about 32 column
+// blocks after stripe t-1), so a tall pair spends the chain length in
+// pipeline fill and drain.  Bands cut the chain into R shorter ones that fill
+// at once; strips multiply the chains of a short pair, so that they fill the
+// GPU.  Column strips are also the per-GPU unit of the multi-GPU split.
 #include <algorithm>
 #include <mutex>
 #include <vector>
@@ -65,6 +70,82 @@ slcs_status side_streams(int count, cudaStream_t *out)
     return SLCS_OK;
 }
 
+struct Perm {
+    int32_t *p;
+    int64_t size;
+};
+
+// One level of a merge tree at a time: in every job's list, neighbours are
+// multiplied (products round robin on the side streams, each stream with its
+// own braid workspace, forked from and joined back to the caller's stream)
+// and an odd last entry is copied; each list is replaced by its products,
+// which are written one after another from `dst`.
+struct Merger {
+    struct Job {
+        std::vector<Perm> *list;
+        int32_t k;     // overlap of every product of the list
+        bool row_glue; // staggered_multiply<true> (bands) or <false> (strips)
+    };
+    cudaStream_t st;
+    cudaStream_t *side;
+    int par;
+    int cutoff;
+    char *ws;
+    size_t ws_bytes;
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[MAX_SIDE] = {};
+
+    slcs_status create()
+    {
+        SLCS_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+        for (int j = 0; j < par; ++j) SLCS_CUDA(cudaEventCreateWithFlags(&join[j], cudaEventDisableTiming));
+        return SLCS_OK;
+    }
+    void destroy()
+    {
+        if (fork) cudaEventDestroy(fork);
+        for (int j = 0; j < par; ++j)
+            if (join[j]) cudaEventDestroy(join[j]);
+    }
+    slcs_status level(std::vector<Job> &jobs, int32_t *dst)
+    {
+        SLCS_CUDA(cudaEventRecord(fork, st));
+        int used = 0, turn = 0;
+        int64_t off = 0;
+        for (Job &J : jobs) {
+            std::vector<Perm> &lv = *J.list;
+            std::vector<Perm> out;
+            for (size_t i = 0; i < lv.size(); i += 2) {
+                if (i + 1 < lv.size()) {
+                    const int j = turn++ % par;
+                    if (j >= used) {
+                        SLCS_CUDA(cudaStreamWaitEvent(side[j], fork, 0));
+                        used = j + 1;
+                    }
+                    const int64_t size = lv[i].size + lv[i + 1].size - J.k;
+                    const slcs_status s = launch_braid(lv[i].p, int(lv[i].size), lv[i + 1].p, int(lv[i + 1].size), J.k,
+                                                       J.row_glue, dst + off, cutoff, ws + ws_bytes * size_t(j),
+                                                       ws_bytes, side[j]);
+                    if (s != SLCS_OK) return s;
+                    out.push_back({dst + off, size});
+                    off += size;
+                } else {
+                    SLCS_CUDA(cudaMemcpyAsync(dst + off, lv[i].p, sizeof(int32_t) * size_t(lv[i].size),
+                                              cudaMemcpyDeviceToDevice, st));
+                    out.push_back({dst + off, lv[i].size});
+                    off += lv[i].size;
+                }
+            }
+            lv.swap(out);
+        }
+        for (int j = 0; j < used; ++j) {
+            SLCS_CUDA(cudaEventRecord(join[j], side[j]));
+            SLCS_CUDA(cudaStreamWaitEvent(st, join[j], 0));
+        }
+        return SLCS_OK;
+    }
+};
+
 } // namespace
 
 int strip_count(const slcs_config *cfg, int32_t n)
@@ -72,6 +153,13 @@ int strip_count(const slcs_config *cfg, int32_t n)
     int s = (cfg && cfg->strips > 0) ? cfg->strips : 8;
     s = std::min(s, std::max(1, int(n / 64)));
     return std::max(1, s);
+}
+
+int band_count(const slcs_config *cfg, int32_t m, int tm)
+{
+    int r = (cfg && cfg->bands > 0) ? cfg->bands : 1;
+    r = std::min(r, std::max(1, int(stripes_of(m, tm))));
+    return std::max(1, r);
 }
 
 std::vector<int32_t> strip_widths(int32_t n, int strips)
@@ -88,6 +176,23 @@ std::vector<int32_t> strip_widths(int32_t n, int strips)
     return w;
 }
 
+std::vector<int32_t> band_heights(int32_t m, int bands, int tm)
+{
+    std::vector<int32_t> h(size_t(bands), 0);
+    if (bands <= 0) return h;
+    // Bands are whole stripes (the last takes the rest), as equal in stripes
+    // as the stripe count allows.
+    const int64_t rows = 32 * int64_t(tm);
+    const int64_t stripes = stripes_of(m, tm);
+    int64_t left = m;
+    for (int r = 0; r < bands; ++r) {
+        const int64_t want = (stripes * (r + 1) / bands - stripes * r / bands) * rows;
+        h[size_t(r)] = int32_t(r + 1 < bands ? std::min(want, left) : left);
+        left -= h[size_t(r)];
+    }
+    return h;
+}
+
 slcs_status perm_to_strands(const int32_t *r2c, int32_t m, int32_t n, int32_t *h, int32_t *v, cudaStream_t st)
 {
     const int64_t size = int64_t(m) + n;
@@ -101,42 +206,56 @@ slcs_status perm_to_strands(const int32_t *r2c, int32_t m, int32_t n, int32_t *h
 slcs_status comb_strips(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n, int32_t *h_out, int32_t *v_out,
                         const slcs_config *cfg, int tm, int warps, cudaStream_t st)
 {
+    const int R = band_count(cfg, m, tm);
     const int S = strip_count(cfg, n);
+    const std::vector<int32_t> hgt = band_heights(m, R, tm);
     const std::vector<int32_t> w = strip_widths(n, S);
-    std::vector<slcs_pair_desc> pd(static_cast<size_t>(S));
-    int64_t b0 = 0, o0 = 0;
-    for (int s = 0; s < S; ++s) {
-        pd[size_t(s)] = slcs_pair_desc{0, b0, o0, m, w[size_t(s)]};
-        b0 += w[size_t(s)];
-        o0 += int64_t(m) + w[size_t(s)];
+    // Tile (r, s) = (band r of a, strip s of b), numbered r * S + s.
+    const int T = R * S;
+    std::vector<slcs_pair_desc> pd(static_cast<size_t>(T));
+    int64_t o0 = 0;
+    {
+        int64_t a0 = 0;
+        for (int r = 0; r < R; ++r) {
+            int64_t b0 = 0;
+            for (int s = 0; s < S; ++s) {
+                pd[size_t(r * S + s)] = slcs_pair_desc{a0, b0, o0, hgt[size_t(r)], w[size_t(s)]};
+                b0 += w[size_t(s)];
+                o0 += int64_t(hgt[size_t(r)]) + w[size_t(s)];
+            }
+            a0 += hgt[size_t(r)];
+        }
     }
-    const int64_t total = o0; // S*m + n strands
-    // Schedule of the wavefront launch: all stripes of all strips.
+    const int64_t total = o0; // S*m + R*n strands
+    // Schedule of the wavefront launch: the stripes of every tile, tile after
+    // tile, so that a stripe's producer is the task before it.
     std::vector<int2> tasks;
-    std::vector<int64_t> scr_off(size_t(S), 0);
+    std::vector<int64_t> scr_off(size_t(T), 0);
     int64_t scr_elems = 0;
-    for (int s = 0; s < S; ++s) {
-        const int32_t st_count = stripes_of(m, tm);
-        for (int32_t k = 0; k < st_count; ++k) tasks.push_back(make_int2(s, k));
-        scr_off[size_t(s)] = scr_elems;
-        scr_elems += scratch_elems(m, w[size_t(s)], tm);
+    for (int t = 0; t < T; ++t) {
+        const int32_t st_count = stripes_of(pd[size_t(t)].m, tm);
+        for (int32_t k = 0; k < st_count; ++k) tasks.push_back(make_int2(t, k));
+        scr_off[size_t(t)] = scr_elems;
+        scr_elems += scratch_elems(pd[size_t(t)].m, pd[size_t(t)].n, tm);
     }
     const int cutoff = (cfg && cfg->braid_cutoff > 0) ? cfg->braid_cutoff : 1024;
-    // Every product of the tree has overlap m and sides of at most m + n.
+    // Products glue strips with overlap = band height and bands with overlap
+    // n; no side exceeds m + n.
     size_t braid_bytes = 0;
-    braid_workspace_bytes(int(int64_t(m) + n), int(int64_t(m) + n), m, cutoff, &braid_bytes);
+    braid_workspace_bytes(int(int64_t(m) + n), int(int64_t(m) + n), std::max(m, n), cutoff, &braid_bytes);
     // Workspace: descriptors, tasks, scratch offsets, counters, scratch,
-    // strands / permutations (two buffers of S*m+n), braid workspace.
+    // strands / permutations (two buffers of S*m+R*n), braid workspaces.
     const size_t o_pairs = 0;
-    const size_t o_tasks = align256(o_pairs + sizeof(PairDev) * size_t(S));
+    const size_t o_tasks = align256(o_pairs + sizeof(PairDev) * size_t(T));
     const size_t o_soff = align256(o_tasks + sizeof(int2) * tasks.size());
-    const size_t o_work = align256(o_soff + sizeof(int64_t) * size_t(S));
+    const size_t o_work = align256(o_soff + sizeof(int64_t) * size_t(T));
     const size_t work_bytes = align256(sizeof(int32_t) * (4 + tasks.size()));
     const size_t o_scr = o_work + work_bytes;
     const size_t o_x = align256(o_scr + sizeof(int32_t) * size_t(scr_elems) + 16);
     const size_t o_y = align256(o_x + sizeof(int32_t) * size_t(total));
     const size_t o_braid = align256(o_y + sizeof(int32_t) * size_t(total));
-    const int par = std::max(1, std::min(MAX_SIDE, S / 2)); // products of a level in flight
+    const int most = std::max(R * (S / 2), R / 2); // products of the widest merge level
+    const int par = std::max(1, std::min(MAX_SIDE, most));
     braid_bytes = align256(braid_bytes);
     const size_t bytes = o_braid + braid_bytes * size_t(par);
     char *ws = nullptr;
@@ -146,10 +265,10 @@ slcs_status comb_strips(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n
         if (s == SLCS_OK && e != cudaSuccess) s = cuda_fail(e, what);
     };
     // Host vectors are pageable: each copy has left them when it returns.
-    cu(cudaMemcpyAsync(ws + o_pairs, pd.data(), sizeof(PairDev) * size_t(S), cudaMemcpyHostToDevice, st), "pairs");
+    cu(cudaMemcpyAsync(ws + o_pairs, pd.data(), sizeof(PairDev) * size_t(T), cudaMemcpyHostToDevice, st), "pairs");
     cu(cudaMemcpyAsync(ws + o_tasks, tasks.data(), sizeof(int2) * tasks.size(), cudaMemcpyHostToDevice, st),
        "tasks");
-    cu(cudaMemcpyAsync(ws + o_soff, scr_off.data(), sizeof(int64_t) * size_t(S), cudaMemcpyHostToDevice, st),
+    cu(cudaMemcpyAsync(ws + o_soff, scr_off.data(), sizeof(int64_t) * size_t(T), cudaMemcpyHostToDevice, st),
        "scratch offsets");
     cu(cudaMemsetAsync(ws + o_work, 0, work_bytes, st), "counters");
     int32_t *X = reinterpret_cast<int32_t *>(ws + o_x);
@@ -170,64 +289,38 @@ slcs_status comb_strips(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n
         L.wait_ns = wait_limit_ns(cfg);
         s = launch_comb(L, tm, warps, st, nullptr);
     }
-    // Strands of every strip -> its permutation (row -> col) in Y.
-    struct Perm {
-        int32_t *p;
-        int64_t size;
-    };
-    std::vector<Perm> level;
-    for (int k = 0; k < S && s == SLCS_OK; ++k) {
-        const int64_t off = pd[size_t(k)].out_offset;
-        s = launch_strands_to_perm(X + off, m, X + off + m, w[size_t(k)], Y + off, nullptr, st);
-        level.push_back({Y + off, int64_t(m) + w[size_t(k)]});
+    // Strands of every tile -> its permutation (row -> col) in Y.
+    std::vector<Perm> tiles;
+    for (int t = 0; t < T && s == SLCS_OK; ++t) {
+        const slcs_pair_desc &d = pd[size_t(t)];
+        s = launch_strands_to_perm(X + d.out_offset, d.m, X + d.out_offset + d.m, d.n, Y + d.out_offset, nullptr, st);
+        tiles.push_back({Y + d.out_offset, int64_t(d.m) + d.n});
     }
-    // Balanced merge tree, ping-ponging between Y and X; the products of a
-    // level run on `par` side streams.
-    int32_t *dst = X;
     cudaStream_t side[MAX_SIDE] = {};
-    if (s == SLCS_OK && S > 1) s = side_streams(par, side);
-    cudaEvent_t fork = nullptr, join[MAX_SIDE] = {};
-    if (s == SLCS_OK && S > 1) {
-        cu(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
-        for (int j = 0; j < par; ++j) cu(cudaEventCreateWithFlags(&join[j], cudaEventDisableTiming), "event");
-    }
-    while (s == SLCS_OK && level.size() > 1) {
-        std::vector<Perm> next;
-        int64_t off = 0;
-        cu(cudaEventRecord(fork, st), "fork");
-        int used = 0;
-        for (size_t i = 0; i < level.size() && s == SLCS_OK; i += 2) {
-            if (i + 1 < level.size()) {
-                const int j = int((i / 2) % size_t(par));
-                if (j >= used) {
-                    cu(cudaStreamWaitEvent(side[j], fork, 0), "fork wait");
-                    used = j + 1;
-                }
-                const int64_t size = level[i].size + level[i + 1].size - m;
-                if (s == SLCS_OK)
-                    s = launch_braid(level[i].p, int(level[i].size), level[i + 1].p, int(level[i + 1].size), m, false,
-                                     dst + off, cutoff, ws + o_braid + braid_bytes * size_t(j), braid_bytes, side[j]);
-                next.push_back({dst + off, size});
-                off += size;
-            } else {
-                cu(cudaMemcpyAsync(dst + off, level[i].p, sizeof(int32_t) * size_t(level[i].size),
-                                   cudaMemcpyDeviceToDevice, st),
-                   "odd strip copy");
-                next.push_back({dst + off, level[i].size});
-                off += level[i].size;
-            }
-        }
-        for (int j = 0; j < used; ++j) {
-            cu(cudaEventRecord(join[j], side[j]), "join");
-            cu(cudaStreamWaitEvent(st, join[j], 0), "join wait");
-        }
-        level.swap(next);
+    if (s == SLCS_OK && T > 1) s = side_streams(par, side);
+    Merger M{st, side, par, cutoff, ws + o_braid, braid_bytes};
+    if (s == SLCS_OK && T > 1) s = M.create();
+    // Strips of every band glue with overlap = band height (column glue),
+    // all bands side by side; then the bands glue with overlap n (row glue).
+    // Each level writes into the buffer the previous one did not.
+    int32_t *dst = X;
+    std::vector<std::vector<Perm>> rows(static_cast<size_t>(R));
+    for (int r = 0; r < R; ++r) rows[size_t(r)].assign(tiles.begin() + r * S, tiles.begin() + (r + 1) * S);
+    while (s == SLCS_OK && rows[0].size() > 1) {
+        std::vector<Merger::Job> jobs;
+        for (int r = 0; r < R; ++r) jobs.push_back({&rows[size_t(r)], hgt[size_t(r)], false});
+        s = M.level(jobs, dst);
         dst = (dst == X) ? Y : X;
     }
-    if (fork) cudaEventDestroy(fork);
-    for (int j = 0; j < par; ++j)
-        if (join[j]) cudaEventDestroy(join[j]);
-    if (s == SLCS_OK) s = perm_to_strands(level[0].p, m, n, h_out, v_out, st);
+    std::vector<Perm> col;
+    for (int r = 0; r < R; ++r) col.push_back(rows[size_t(r)][0]);
+    while (s == SLCS_OK && col.size() > 1) {
+        std::vector<Merger::Job> jobs{{&col, n, true}};
+        s = M.level(jobs, dst);
+        dst = (dst == X) ? Y : X;
+    }
+    M.destroy();
+    if (s == SLCS_OK) s = perm_to_strands(col[0].p, m, n, h_out, v_out, st);
     cudaFreeAsync(ws, st);
     return s;
 }

@@ -30,8 +30,8 @@ class Config(ctypes.Structure):
     _fields_ = [("algo", ctypes.c_int32), ("tile_m", ctypes.c_int32), ("tile_n", ctypes.c_int32),
                 ("warps", ctypes.c_int32), ("braid_cutoff", ctypes.c_int32), ("strips", ctypes.c_int32),
                 ("use_graph", ctypes.c_int32), ("seg", ctypes.c_int32), ("wait_ms", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32), ("strand_bits", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 5)]
+                ("blocks_per_sm", ctypes.c_int32), ("strand_bits", ctypes.c_int32), ("bands", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 4)]
 
     @classmethod
     def make(cls, **kw) -> "Config":
@@ -52,6 +52,15 @@ class PlanInfo(ctypes.Structure):
                 ("warps", ctypes.c_int32), ("stream_pairs", ctypes.c_int32), ("wavefront_tasks", ctypes.c_int32),
                 ("stream_classes", ctypes.c_int32), ("tile_n", ctypes.c_int32), ("grid", ctypes.c_int32),
                 ("packed_pairs", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
+
+
+class PairInfo(ctypes.Structure):
+    _fields_ = [("algo", ctypes.c_int32), ("tile_m", ctypes.c_int32), ("warps", ctypes.c_int32),
+                ("strips", ctypes.c_int32), ("bands", ctypes.c_int32), ("braid_cutoff", ctypes.c_int32),
+                ("stripes", ctypes.c_int32), ("reserved", ctypes.c_int32 * 9)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
@@ -90,6 +99,7 @@ def lib():
         L.slcs_batch_plan_launches.argtypes = [_vp]
         L.slcs_batch_plan_launches.restype = _i32
         L.slcs_batch_plan_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
+        L.slcs_pair_plan_info.argtypes = [_i32, _i32, ctypes.POINTER(Config), ctypes.POINTER(PairInfo)]
         L.slcs_strands_to_permutation.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, _vp]
         L.slcs_permutation_to_strands.argtypes = [_vp, _i32, _i32, _vp, _vp, _vp]
         L.slcs_substring_llcs.argtypes = [_vp, _i32, _i32, _vp, _vp, _i32, _vp, _vp]
@@ -143,6 +153,14 @@ def comb_pair(a, b, cfg: Optional[Config] = None, stream=None, out=None):
     check(lib().slcs_comb_pair(_dptr(a), m, _dptr(b), n, _dptr(out), _dptr(out) + 4 * m if n else 0,
                                _cfg(cfg), _stream(stream)))
     return h, v
+
+
+def pair_plan_info(m: int, n: int, cfg: Optional[Config] = None) -> dict:
+    """How comb_pair combs an m x n pair under cfg (kernel family, rows per
+    lane, warps, strips, bands, braid cutoff, stripes); launches nothing."""
+    pi = PairInfo()
+    check(lib().slcs_pair_plan_info(int(m), int(n), _cfg(cfg), ctypes.byref(pi)))
+    return pi.as_dict()
 
 
 def comb_pair_host(a: np.ndarray, b: np.ndarray, cfg: Optional[Config] = None):

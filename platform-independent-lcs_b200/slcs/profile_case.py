@@ -40,7 +40,7 @@ def main():
         a = torch.from_numpy(rng.integers(0, 4, n, dtype=np.uint8)).to(dev)
         b = torch.from_numpy(rng.integers(0, 4, n, dtype=np.uint8)).to(dev)
         out = torch.empty(2 * n, dtype=torch.int32, device=dev)
-        cfg = slcs.Config.make(tile_m=tm or 16, wait_ms=600000)
+        cfg = slcs.Config.make(tile_m=tm or None, wait_ms=600000)  # tm 0: the library's rule
         for _ in range(2):
             slcs.comb_pair(a, b, cfg=cfg, out=out)
         torch.cuda.synchronize()

@@ -90,8 +90,8 @@ def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev, sampler=None):
     ad = torch.from_numpy(a).to(dev)
     bd = torch.from_numpy(b).to(dev)
     o = torch.empty(len(a) + len(b), dtype=torch.int32, device=dev)
-    from . import comb_pair
-    cfg = Config.make()  # default rule: 16 rows per lane, 8 warps per block at this height
+    from . import comb_pair, pair_plan_info
+    cfg = Config.make()  # the library's default rule for a pair of this height
     comb_pair(ad, bd, cfg=cfg, out=o)
     torch.cuda.synchronize()
     runs = []
@@ -119,7 +119,8 @@ def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev, sampler=None):
     res["long_pair"] = {"workload": "pair_1M (1048576 x 1048576, uniform {0..3})", "ms": ms, "gcups": g,
                         "roofline_frac": g / roof_gcups, "hash": hv,
                         "bitexact_vs_reference": (hv == gold) if gold is not None else None,
-                        "variant": {"tile_m": 16, "warps": 8}, "runs_ms": runs,
+                        "variant": pair_plan_info(len(a), len(b), cfg),
+                        "runs_ms": runs,
                         "clocks": smp.summary() if smp else None}
     res.update(strips_and_braid(ad, bd, o, gold, dev))
     return res
@@ -134,11 +135,12 @@ def _measured_hbm_gbs():
 
 
 def strips_and_braid(ad, bd, o, gold_hash, dev):
-    """The 2^20 x 2^20 pair as 8 column strips glued by braid products, over
-    the cutoff sweep {64, 256, 1024, 4096}; and one braid product alone (the
-    top merge of the two halves of b, overlap k = 2^20) against HBM."""
+    """The 2^20 x 2^20 pair in the default tiling (row bands glued by
+    row-glue braid products) over the cutoff sweep {64, 256, 1024, 4096}; and
+    one braid product alone (the top merge of the two halves of b, overlap
+    k = 2^20) against HBM."""
     import torch
-    from . import braid_multiply, comb_pair
+    from . import braid_multiply, comb_pair, pair_plan_info
     st = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     m, n = int(ad.numel()), int(bd.numel())
@@ -158,7 +160,7 @@ def strips_and_braid(ad, bd, o, gold_hash, dev):
 
     sweep = {}
     for cutoff in (64, 256, 1024, 4096):
-        cfg = Config.make(algo=2, strips=8, braid_cutoff=cutoff)
+        cfg = Config.make(braid_cutoff=cutoff)
         ms = timed(lambda: comb_pair(ad, bd, cfg=cfg, out=o))
         _, c2r = strands_to_permutation(o[:m], o[m:])
         hv = permutation_hash(c2r.cpu().numpy())
@@ -178,6 +180,8 @@ def strips_and_braid(ad, bd, o, gold_hash, dev):
         algo_bytes = 4 * (p + q) + 4 * (p + q - m)
         gbs = algo_bytes / (ms * 1e-3) / 1e9
         braid[str(cutoff)] = {"ms": ms, "algorithmic_bytes": algo_bytes, "achieved_gbs": gbs, "frac": gbs / peak}
-    return {"long_pair_strips": {"workload": "pair_1M as 8 column strips + braid merge tree", "cutoff_sweep": sweep},
+    tiles = pair_plan_info(m, n)
+    return {"long_pair_tiles": {"workload": f"pair_1M as {tiles['bands']} row bands x {tiles['strips']} column "
+                                             "strips + braid merge trees", "cutoff_sweep": sweep},
             "braid_top_merge": {"workload": "staggered_multiply<false>(P(a,b[:n/2]), P(a,b[n/2:]), k=2^20)",
                                 "bound": "hbm", "peak_gbs": peak, "peak_source": peak_src, "by_cutoff": braid}}

@@ -317,7 +317,8 @@ def _sha256(x):
 
 
 @pytest.mark.parametrize("name,cfg", [("pair_131072_mutated", dict()),
-                                      ("pair_1M", dict(tile_m=16, warps=8))])
+                                      ("pair_1M", dict(tile_m=16, warps=8)),
+                                      ("pair_1M", dict())])
 def test_pair_large_golden(cuda, name, cfg):
     """Full-size single pairs against digests of the oracle's permutation
     (tests/golden/make_golden.py --big wrote them)."""
