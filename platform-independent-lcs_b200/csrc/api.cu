@@ -691,6 +691,7 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
             if (pack)
                 for (int t : {4, 8, 12, 16}) P->classes.push_back({t, 16, true});
             for (int t : {4, 8, 12, 16}) P->classes.push_back({t, 16, false});
+            P->classes.push_back({12, 32, false});
             P->classes.push_back({16, 32, false});
         }
         for (const auto &c : P->classes)
@@ -788,7 +789,13 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
         for (int c = 0; c < nclass; ++c) sum_wmax += wmax[c];
         want = std::max(want, (sum_wmax + BATCH_WARPS - 1) / BATCH_WARPS);
         grid = int(std::max<long>(1, std::min<long>(grid, want)));
-        const long warps_total = long(grid) * BATCH_WARPS;
+        // One warp per wavefront task gets no stream list: those warps take
+        // the tasks from the start, so the stripe chains of the tall pairs
+        // run under the stream work instead of after it (a 3-stripe chain of
+        // 800 columns alone on a drained GPU took ~50 us, about an eighth of
+        // the 20,000-read launch).
+        const long reserve = std::min<long>(P->ntasks, long(grid) * BATCH_WARPS / 8);
+        const long warps_total = long(grid) * BATCH_WARPS - reserve;
         std::vector<long> wc(nclass, 0);
         long used = 0;
         for (int c = 0; c < nclass; ++c) {
