@@ -4,16 +4,25 @@ Batches of independent pairs shard without any exchange: shard_pairs() deals
 the pairs out longest first to the rank with the fewest cells so far, and each
 rank combs its shard with its own batch plan.
 
-One long pair splits by columns of b.  Rank g combs the strip (a, b_g), turns
-its strands into the permutation P(a, b_g), and a binary tree of sticky-braid
-products with overlap m glues the strips back together
-(staggered_multiply<false>(P(a, x), P(a, y), m) == P(a, x y),
-src/braid_multiplication.hpp:273-407): in round r, rank g with
-g % 2^(r+1) == 0 receives the permutation of rank g + 2^r by point-to-point
-send/recv -- the peer's array lands in this GPU's own memory before the
-product kernel reads it -- and multiplies.  Rank 0 ends with P(a, b) and
-returns its strands.  Strip widths follow the library's strip mode, so one
-GPU in strip mode and G GPUs produce the same products.
+One long pair splits into G parts, one per rank, either by rows of a (bands)
+or by columns of b (strips).  Rank g combs its part, turns the strands into
+the part's permutation, and a binary tree of sticky-braid products glues the
+parts back together (src/braid_multiplication.hpp:273-407):
+
+    bands:  staggered_multiply<true>(P(x, b), P(y, b), n)  == P(x y, b)
+    strips: staggered_multiply<false>(P(a, x), P(a, y), m) == P(a, x y)
+
+In round r, rank g with g % 2^(r+1) == 0 receives the permutation of rank
+g + 2^r by point-to-point send/recv -- the peer's array lands in this GPU's
+own memory before the product kernel reads it -- and multiplies.  Rank 0 ends
+with P(a, b) and returns its strands.  Bands are the default for pairs at
+least as tall as they are wide: the stripes of one comb form a chain whose
+fill and drain grow with the rows, so G bands of m/G rows each fill G times
+faster than G strips of full height (on one B200 the 2^20 x 2^20 pair combs
+in 324 ms as 8 bands and 677-729 ms as 8 strips).  Strip widths follow the
+library's tile mode (multiples of 16 columns); band heights are whole stripes
+of 448 rows (14 rows per lane, the library's choice for the tallest pairs).
+Any heights and widths give the same strands.
 
 The compute steps go through a kernels object (CudaKernels: the library's C
 ABI).  The exchange logic does not depend on what computes, which is how it
@@ -38,6 +47,21 @@ def strip_widths(n: int, strips: int) -> List[int]:
         w = min(base, left) if s + 1 < strips else left
         out.append(w)
         left -= w
+    return out
+
+
+def band_heights(m: int, bands: int, rows_per_stripe: int = 448) -> List[int]:
+    """Heights of `bands` row bands of m rows, top to bottom: whole stripes of
+    `rows_per_stripe` rows, as equal in stripes as the stripe count allows;
+    the last band takes the rest."""
+    bands = max(1, int(bands))
+    stripes = (m + rows_per_stripe - 1) // rows_per_stripe if m > 0 else 0
+    out, left = [], m
+    for r in range(bands):
+        want = (stripes * (r + 1) // bands - stripes * r // bands) * rows_per_stripe
+        h = min(want, left) if r + 1 < bands else left
+        out.append(h)
+        left -= h
     return out
 
 
@@ -78,9 +102,9 @@ class CudaKernels:
         from . import strands_to_permutation
         return strands_to_permutation(h, v)[0]
 
-    def braid(self, p, q, k):
+    def braid(self, p, q, k, row_glue=False):
         from . import braid_multiply
-        return braid_multiply(p, q, k, False, cfg=self.cfg)
+        return braid_multiply(p, q, k, row_glue, cfg=self.cfg)
 
     def to_strands(self, r2c, m):
         from . import permutation_to_strands
@@ -91,22 +115,32 @@ class CudaKernels:
         return torch.empty(int(size), dtype=torch.int32, device=like.device)
 
 
-def comb_pair_distributed(a, b, group=None, kernels=None):
+def comb_pair_distributed(a, b, group=None, kernels=None, split: str = "auto"):
     """Strands (h, v) of one pair on rank 0 (None on the other ranks).
 
     a and b are the whole strings on every rank (uint8 tensors on this rank's
-    device); each rank reads only its strip of b.  Every rank takes the same
-    send/recv steps in the same order."""
+    device); each rank reads only its band of a or strip of b.  split is
+    "bands", "strips" or "auto" (bands when m >= n).  Every rank takes the
+    same send/recv steps in the same order."""
     import torch.distributed as dist
     K = kernels or CudaKernels()
     rank = dist.get_rank(group)
     world = dist.get_world_size(group)
     m, n = int(a.numel()), int(b.numel())
-    widths = strip_widths(n, world)
-    start = sum(widths[:rank])
-    h, v = K.comb(a, b[start:start + widths[rank]])
+    if split == "auto":
+        split = "bands" if m >= n else "strips"
+    if split not in ("bands", "strips"):
+        raise ValueError("split must be 'bands', 'strips' or 'auto'")
+    rows = split == "bands"
+    parts = band_heights(m, world) if rows else strip_widths(n, world)
+    start = sum(parts[:rank])
+    if rows:
+        h, v = K.comb(a[start:start + parts[rank]], b)
+    else:
+        h, v = K.comb(a, b[start:start + parts[rank]])
     P = K.to_perm(h, v)
-    sizes = [m + w for w in widths]  # current permutation size held by each rank
+    k = n if rows else m  # overlap of every product
+    sizes = [p + k for p in parts]  # current permutation size held by each rank
     for rnd in merge_rounds(world):
         for dst, src in rnd:
             if rank == src:
@@ -114,9 +148,9 @@ def comb_pair_distributed(a, b, group=None, kernels=None):
             elif rank == dst:
                 Q = K.empty(sizes[src], P)
                 dist.recv(Q, group=group, group_src=src)
-                P = K.braid(P, Q, m)
+                P = K.braid(P, Q, k, rows)
         for dst, src in rnd:
-            sizes[dst] = sizes[dst] + sizes[src] - m
+            sizes[dst] = sizes[dst] + sizes[src] - k
     if rank != 0:
         return None
     return K.to_strands(P, m)

@@ -23,6 +23,14 @@ def test_strip_widths():
             assert all(w[i] % 16 == 0 or sum(w[i + 1:]) == 0 for i in range(s - 1))
 
 
+def test_band_heights():
+    for m in (0, 1, 447, 448, 449, 5000, 1 << 20):
+        for bands in (1, 2, 3, 8):
+            h = D.band_heights(m, bands)
+            assert len(h) == bands and sum(h) == m and min(h) >= 0
+            assert all(x % 448 == 0 for x in h[:-1])
+
+
 def test_merge_rounds_cover_every_rank_once():
     for world in range(1, 9):
         alive = set(range(world))
@@ -55,9 +63,9 @@ class OracleKernels:
         import torch
         return torch.from_numpy(O.from_strands(h.numpy(), v.numpy())[0])
 
-    def braid(self, p, q, k):
+    def braid(self, p, q, k, row_glue=False):
         import torch
-        return torch.from_numpy(O.staggered_multiply(p.numpy(), q.numpy(), k, False)[0])
+        return torch.from_numpy(O.staggered_multiply(p.numpy(), q.numpy(), k, row_glue)[0])
 
     def to_strands(self, r2c, m):
         import torch
@@ -75,7 +83,7 @@ class OracleKernels:
         return torch.empty(int(size), dtype=torch.int32)
 
 
-def _worker(rank, world, port, m, n, seed, out_path):
+def _worker(rank, world, port, m, n, seed, out_path, split):
     import torch
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -85,7 +93,7 @@ def _worker(rank, world, port, m, n, seed, out_path):
         rng = np.random.default_rng(seed)
         a = torch.from_numpy(rng.integers(0, 4, m, dtype=np.uint8))
         b = torch.from_numpy(rng.integers(0, 4, n, dtype=np.uint8))
-        res = D.comb_pair_distributed(a, b, kernels=OracleKernels())
+        res = D.comb_pair_distributed(a, b, kernels=OracleKernels(), split=split)
         if rank == 0:
             np.savez(out_path, h=res[0].numpy(), v=res[1].numpy())
         else:
@@ -94,8 +102,9 @@ def _worker(rank, world, port, m, n, seed, out_path):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,m,n", [(2, 300, 1000), (3, 257, 777), (2, 100, 20)])
-def test_comb_pair_distributed_gloo(world, m, n):
+@pytest.mark.parametrize("world,m,n,split", [(2, 300, 1000, "strips"), (3, 257, 777, "strips"), (2, 100, 20, "auto"),
+                                             (2, 1000, 300, "bands"), (3, 1500, 257, "auto"), (2, 5, 40, "bands")])
+def test_comb_pair_distributed_gloo(world, m, n, split):
     import socket
 
     import torch.multiprocessing as mp
@@ -105,7 +114,7 @@ def test_comb_pair_distributed_gloo(world, m, n):
     seed = 17 + world + m
     with tempfile.TemporaryDirectory() as d:
         out = os.path.join(d, "res.npz")
-        mp.start_processes(_worker, args=(world, port, m, n, seed, out), nprocs=world, join=True,
+        mp.start_processes(_worker, args=(world, port, m, n, seed, out, split), nprocs=world, join=True,
                            start_method="spawn")
         got = np.load(out)
         rng = np.random.default_rng(seed)
