@@ -58,6 +58,7 @@ SemiLocalLcsImpl LcsAlgorithmRegistry::Get(std::string name, std::string device_
 #define SLCS_SEMI2(name, fn) reg2[name] = fn;
 #define SLCS_WAVEFRONT(TM, W) SLCS_SEMI2("b200_" #TM "_" #W, (Lcs_Semi_B200_Wavefront<TM, W>))
 #define SLCS_STRIPS(S, CUT) SLCS_SEMI2("b200_strips_" #S "_" #CUT, (Lcs_Semi_B200_Strips<S, CUT>))
+#define SLCS_BANDS(R, CUT) SLCS_SEMI2("b200_bands_" #R "_" #CUT, (Lcs_Semi_B200_Bands<R, CUT>))
 
 LcsAlgorithmRegistry::LcsAlgorithmRegistry()
 {
@@ -66,10 +67,13 @@ LcsAlgorithmRegistry::LcsAlgorithmRegistry()
     SLCS_WAVEFRONT(4, 2) SLCS_WAVEFRONT(4, 4) SLCS_WAVEFRONT(4, 8)
     SLCS_WAVEFRONT(8, 2) SLCS_WAVEFRONT(8, 4) SLCS_WAVEFRONT(8, 8)
     SLCS_WAVEFRONT(12, 2) SLCS_WAVEFRONT(12, 4) SLCS_WAVEFRONT(12, 8)
+    SLCS_WAVEFRONT(14, 4) SLCS_WAVEFRONT(14, 8)
     SLCS_WAVEFRONT(16, 2) SLCS_WAVEFRONT(16, 4) SLCS_WAVEFRONT(16, 8)
     // column strips glued by braid products, over the cutoff sweep
     SLCS_STRIPS(2, 1024) SLCS_STRIPS(4, 1024) SLCS_STRIPS(8, 64) SLCS_STRIPS(8, 256)
     SLCS_STRIPS(8, 1024) SLCS_STRIPS(8, 4096) SLCS_STRIPS(16, 1024)
+    // row bands glued by row-glue braid products
+    SLCS_BANDS(2, 256) SLCS_BANDS(4, 256) SLCS_BANDS(8, 256) SLCS_BANDS(16, 256)
 }
 
 LcsAlgorithmRegistry::~LcsAlgorithmRegistry() = default;

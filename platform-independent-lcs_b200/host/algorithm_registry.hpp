@@ -5,7 +5,8 @@
 // LcsAlgorithmRegistry::Get(name, device_type) returns a SemiLocalLcsImpl whose
 // operator() runs the procedure and builds the PermutationMatrix.  The B200
 // procedures are registered under "b200" and name-encoded variants
-// ("b200_<tile_m>_<warps>", "b200_strips_<strips>_<cutoff>"); device types are
+// ("b200_<tile_m>_<warps>", "b200_strips_<strips>_<cutoff>",
+// "b200_bands_<bands>_<cutoff>"); device types are
 // "gpu" (CUDA device 0) and "cuda:<n>".
 #pragma once
 

@@ -55,6 +55,7 @@ void Lcs_Semi_B200_With(LcsProblemContext &ctx, const B200Variant &variant)
     cfg.warps = variant.warps;
     cfg.strips = variant.strips;
     cfg.braid_cutoff = variant.braid_cutoff;
+    cfg.bands = variant.bands;
     if (ctx.queue && slcs_set_device(ctx.queue->device()) != SLCS_OK) throw std::runtime_error(slcs_last_error());
     std::vector<int32_t> h(m), v(n);
     slcs_status s = slcs_comb_pair_host(a.data(), m, b.data(), n, h.data(), v.data(), &cfg);

@@ -13,6 +13,7 @@ struct B200Variant
     int warps;
     int strips;
     int braid_cutoff;
+    int bands;
 };
 
 // Combs ctx.a_given x ctx.b_given on the CUDA device of ctx.queue and stores
@@ -26,11 +27,18 @@ void Lcs_Semi_B200(LcsProblemContext &ctx);
 template <int TILE_M, int WARPS>
 void Lcs_Semi_B200_Wavefront(LcsProblemContext &ctx)
 {
-    Lcs_Semi_B200_With(ctx, B200Variant{1, TILE_M, WARPS, 0, 0});
+    Lcs_Semi_B200_With(ctx, B200Variant{1, TILE_M, WARPS, 0, 0, 0});
 }
 
 template <int STRIPS, int CUTOFF>
 void Lcs_Semi_B200_Strips(LcsProblemContext &ctx)
 {
-    Lcs_Semi_B200_With(ctx, B200Variant{2, 0, 0, STRIPS, CUTOFF});
+    Lcs_Semi_B200_With(ctx, B200Variant{2, 0, 0, STRIPS, CUTOFF, 0});
+}
+
+// Row bands of a glued by row-glue braid products (one column strip).
+template <int BANDS, int CUTOFF>
+void Lcs_Semi_B200_Bands(LcsProblemContext &ctx)
+{
+    Lcs_Semi_B200_With(ctx, B200Variant{2, 0, 0, 1, CUTOFF, BANDS});
 }

@@ -17,7 +17,7 @@ BIN = os.path.join(ROOT, "platform-independent-lcs_b200", "bin", "slcs_test")
 def test_script_runner_matches_golden_hashes(tmp_path):
     with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
         cases = json.load(f)["test_default"]
-    algos = ["b200", "b200_2_4", "b200_16_8", "b200_strips_4_1024", "b200_strips_8_64"]
+    algos = ["b200", "b200_2_4", "b200_14_8", "b200_16_8", "b200_strips_4_1024", "b200_strips_8_64", "b200_bands_4_256"]
     lines = []
     for alg in algos:
         for c in cases:
