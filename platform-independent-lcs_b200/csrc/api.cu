@@ -475,6 +475,7 @@ slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_
     L.single.b_off = 0;
     L.single.m = m;
     L.single.n = n;
+    L.tw = pick_tw(tm, ntasks, n, b);
     // h and v may live in separate allocations: address v relative to h.
     L.single.out_off = 0;
     slcs_status s;

@@ -90,9 +90,8 @@ __device__ __forceinline__ void cell(int a_sym, int b_sym, int &h, int &v)
 
 // One row stripe of one pair, combed by one warp.  TW columns form a block,
 // the unit of a step, of a scratch-row transfer and of the shuffle hand-off;
-// the ring holds RING blocks of TW strands per warp.  The kernels use TW = 4:
-// 8 columns per step passed the same parity tests but combed the 2^20 pair
-// about 20 % slower.
+// the ring holds RING blocks of TW strands per warp.  TW = 4 everywhere but
+// in launches that pick_tw() gives 8 (short stripe chains of tall tiles).
 template <int TM, int TW>
 struct Stripe {
     static constexpr int Q = TW / 4;                 // int4 per block
@@ -309,10 +308,10 @@ __device__ __forceinline__ void task_of(const CombLaunch &L, int k, PairDev &P, 
 // w * gridDim.x + b in a cooperative launch, spreads consecutive stripes over
 // the SMs; it combed the 2^20 pair in 763 ms instead of 407 ms, because the
 // four stripes sharing a sub-partition then start and finish far apart.)
-template <int TM, int WARPS>
+template <int TM, int WARPS, int TW>
 __global__ void __launch_bounds__(WARPS * 32) comb_wavefront_kernel(const CombLaunch L)
 {
-    __shared__ __align__(16) int4 ring[WARPS][RING];
+    __shared__ __align__(16) int4 ring[WARPS][RING * TW / 4];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     PairDev P;
@@ -324,7 +323,7 @@ __global__ void __launch_bounds__(WARPS * 32) comb_wavefront_kernel(const CombLa
         k = __shfl_sync(FULL_MASK, k, 0);
         if (k >= L.ntasks) break;
         task_of(L, k, P, stripe, so);
-        comb_stripe<TM>(L, P, so, stripe, k, ring[w], lane);
+        comb_stripe<TM, TW>(L, P, so, stripe, k, ring[w], lane);
     }
 }
 
@@ -762,7 +761,7 @@ struct Balanced {
     int smem = 0;
 };
 
-template <int TM>
+template <int TM, int TW>
 slcs_status balanced_setup(Balanced &B)
 {
     int dev = 0, per_sm = 0, optin = 0;
@@ -770,13 +769,13 @@ slcs_status balanced_setup(Balanced &B)
     SLCS_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     SLCS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     cudaFuncAttributes fa{};
-    SLCS_CUDA(cudaFuncGetAttributes(&fa, comb_wavefront_kernel<TM, WF_SM_WARPS>));
+    SLCS_CUDA(cudaFuncGetAttributes(&fa, comb_wavefront_kernel<TM, WF_SM_WARPS, TW>));
     const int want = per_sm / 2 + 1024 - int(fa.sharedSizeBytes);
     if (want <= 0 || want + int(fa.sharedSizeBytes) > optin) return SLCS_OK;
-    SLCS_CUDA(cudaFuncSetAttribute(comb_wavefront_kernel<TM, WF_SM_WARPS>,
+    SLCS_CUDA(cudaFuncSetAttribute(comb_wavefront_kernel<TM, WF_SM_WARPS, TW>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, want));
     int occ = 0;
-    SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WF_SM_WARPS>,
+    SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WF_SM_WARPS, TW>,
                                                             WF_SM_WARPS * 32, size_t(want)));
     B.smem = want;
     B.ok = occ == 1;
@@ -784,7 +783,7 @@ slcs_status balanced_setup(Balanced &B)
 }
 
 // Launches the balanced form when it applies; *done tells whether it did.
-template <int TM>
+template <int TM, int TW>
 slcs_status launch_balanced(const CombLaunch &L, long sms, cudaStream_t stream, int *grid_out, bool *done)
 {
     static Balanced B;
@@ -794,7 +793,7 @@ slcs_status launch_balanced(const CombLaunch &L, long sms, cudaStream_t stream, 
     {
         std::lock_guard<std::mutex> g(mu);
         if (state < 0) {
-            const slcs_status s = balanced_setup<TM>(B);
+            const slcs_status s = balanced_setup<TM, TW>(B);
             if (s != SLCS_OK) return s;
             state = 1;
         }
@@ -805,25 +804,25 @@ slcs_status launch_balanced(const CombLaunch &L, long sms, cudaStream_t stream, 
     *done = true;
     if (stream == PREPARE_ONLY) return SLCS_OK;
     const long grid = std::min<long>(sms, L.ntasks);
-    comb_wavefront_kernel<TM, WF_SM_WARPS><<<int(grid), int(per_sm) * 32, size_t(B.smem), stream>>>(L);
+    comb_wavefront_kernel<TM, WF_SM_WARPS, TW><<<int(grid), int(per_sm) * 32, size_t(B.smem), stream>>>(L);
     if (grid_out) *grid_out = int(grid);
     SLCS_CUDA(cudaGetLastError());
     return SLCS_OK;
 }
 
-template <int TM, int WARPS>
-slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_out)
+template <int TM, int WARPS, int TW>
+slcs_status launch_variant_tw(const CombLaunch &L, cudaStream_t stream, int *grid_out)
 {
     const long sms = sm_count();
     bool done = false;
-    const slcs_status bs = launch_balanced<TM>(L, sms, stream, grid_out, &done);
+    const slcs_status bs = launch_balanced<TM, TW>(L, sms, stream, grid_out, &done);
     if (bs != SLCS_OK || done) return bs;
     static int occ = -1;
     static std::mutex mu;
     {
         std::lock_guard<std::mutex> g(mu);
         if (occ < 0) {
-            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WARPS>,
+            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WARPS, TW>,
                                                                     WARPS * 32, 0));
             if (occ < 1) occ = 1;
         }
@@ -838,10 +837,19 @@ slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_o
     long grid = sms * occ;
     if (want < grid) grid = want;
     if (grid < 1) grid = 1;
-    comb_wavefront_kernel<TM, WARPS><<<int(grid), WARPS * 32, 0, stream>>>(L);
+    comb_wavefront_kernel<TM, WARPS, TW><<<int(grid), WARPS * 32, 0, stream>>>(L);
     if (grid_out) *grid_out = int(grid);
     SLCS_CUDA(cudaGetLastError());
     return SLCS_OK;
+}
+
+template <int TM, int WARPS>
+slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_out)
+{
+    if constexpr (TM == 14 || TM == 16) {
+        if (L.tw == 8) return launch_variant_tw<TM, WARPS, 8>(L, stream, grid_out);
+    }
+    return launch_variant_tw<TM, WARPS, 4>(L, stream, grid_out);
 }
 
 template <int TNS, int WARPS>
@@ -875,14 +883,14 @@ template <int TM, int WARPS>
 slcs_status launch_variant_on(const CombLaunch &L, int sms, cudaStream_t stream)
 {
     bool done = false;
-    const slcs_status bs = launch_balanced<TM>(L, sms, stream, nullptr, &done);
+    const slcs_status bs = launch_balanced<TM, 4>(L, sms, stream, nullptr, &done);
     if (bs != SLCS_OK || done) return bs;
     static int occ = -1;
     static std::mutex mu;
     {
         std::lock_guard<std::mutex> g(mu);
         if (occ < 0) {
-            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WARPS>,
+            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WARPS, 4>,
                                                                     WARPS * 32, 0));
             if (occ < 1) occ = 1;
         }
@@ -891,7 +899,7 @@ slcs_status launch_variant_on(const CombLaunch &L, int sms, cudaStream_t stream)
     long grid = long(sms > 0 ? sms : 1) * occ;
     if (want < grid) grid = want;
     if (grid < 1) grid = 1;
-    comb_wavefront_kernel<TM, WARPS><<<int(grid), WARPS * 32, 0, stream>>>(L);
+    comb_wavefront_kernel<TM, WARPS, 4><<<int(grid), WARPS * 32, 0, stream>>>(L);
     SLCS_CUDA(cudaGetLastError());
     return SLCS_OK;
 }

@@ -23,7 +23,20 @@ struct CombLaunch {
     uint32_t *status;           // mapped device status word
     uint64_t wait_ns;           // limit of one bounded wait
     PairDev single;
+    int32_t tw;                 // wavefront columns per step: 8 (tile_m 14/16 only) or 4 (0 = 4)
 };
+
+// Columns per step for a wavefront launch whose longest stripe chain has
+// `chain` stripes and whose narrowest tile has `width` columns of b: 8 halves
+// the per-step work of a stripe outside the cells but doubles the columns a
+// chain spends filling, so it pays only while the chain is short against the
+// width (2^20-column bands of 147-585 stripes: 1.8-4.6 % faster; one chain of
+// 2341 stripes: 21 % slower).  The 8-byte symbol loads need b 8-byte aligned.
+inline int32_t pick_tw(int tm, int64_t chain, int64_t width, const void *b)
+{
+    const bool aligned = (reinterpret_cast<uintptr_t>(b) & 7) == 0;
+    return ((tm == 14 || tm == 16) && aligned && chain * 2000 <= width) ? 8 : 4;
+}
 
 // A batch launch: multi-stripe pairs go through the wavefront tasks above
 // (whole warps, tile_m rows per lane), then every single-stripe pair is

@@ -287,6 +287,12 @@ slcs_status comb_strips(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n
         L.progress = L.counters + 4;
         L.status = device_status_word();
         L.wait_ns = wait_limit_ns(cfg);
+        int64_t chain = 0, width = INT64_MAX;
+        for (const slcs_pair_desc &d : pd) {
+            chain = std::max<int64_t>(chain, stripes_of(d.m, tm));
+            width = std::min<int64_t>(width, d.n);
+        }
+        L.tw = pick_tw(tm, chain, width, b);
         s = launch_comb(L, tm, warps, st, nullptr);
     }
     // Strands of every tile -> its permutation (row -> col) in Y.

@@ -38,12 +38,14 @@ def test_pair_shapes(cuda, tm):
         _check_pair(a, b, cuda, slcs.Config.make(tile_m=tm))
 
 
-@pytest.mark.parametrize("tm,m,n", [(2, 160000, 333), (14, 7 * 448 + 5, 1001), (16, 64 * 512 + 1, 97)])
+@pytest.mark.parametrize("tm,m,n", [(2, 160000, 333), (14, 7 * 448 + 5, 1001), (16, 64 * 512 + 1, 97),
+                                    (16, 1000, 9001), (14, 900, 6007)])
 def test_pair_stripe_counts(cuda, tm, m, n):
     """Stripe counts around the resident capacity: 2500 stripes of 64 rows are
     more than one launch holds at once (persistent blocks take stripes from the
     ticket counter); the others run one block per SM, the last one with a
-    single-row stripe at the bottom."""
+    single-row stripe at the bottom; the last two are short chains against
+    their width, combed 8 columns per step (ragged last block)."""
     rng = np.random.default_rng(m + n)
     a = rng.integers(0, 4, m, dtype=np.uint8)
     b = rng.integers(0, 4, n, dtype=np.uint8)

@@ -83,10 +83,13 @@ def test_default_rule_picks_strips_and_matches(cuda, m, n):
 
 @pytest.mark.parametrize("m,n,bands,strips,tm,cutoff", [
     (3000, 2000, 2, 1, 4, 0), (5000, 1500, 3, 2, 8, 64), (4097, 333, 5, 1, 2, 256),
-    (64, 5000, 4, 3, 2, 0), (10000, 1, 4, 1, 4, 0), (7000, 7000, 16, 2, 14, 1024), (1, 1, 2, 2, 2, 0)])
+    (64, 5000, 4, 3, 2, 0), (10000, 1, 4, 1, 4, 0), (7000, 7000, 16, 2, 14, 1024), (1, 1, 2, 2, 2, 0),
+    (20000, 10007, 8, 1, 16, 0)])
 def test_bands_match_direct_comb(cuda, m, n, bands, strips, tm, cutoff):
     """Row bands (whole stripes of 32*tm rows; more bands than stripes are
-    capped) and strips together, including n = 1 (row-glue overlap 1)."""
+    capped) and strips together, including n = 1 (row-glue overlap 1) and
+    tiles short enough against their width for 8 columns per step (7000^2 in
+    16 x 2 tiles, 20000 x 10007 in 8 bands: ragged last block)."""
     rng = np.random.default_rng(m * 3 + n + bands)
     sigma = int(rng.choice([2, 4, 20]))
     a = rng.integers(0, sigma, m, dtype=np.uint8)
