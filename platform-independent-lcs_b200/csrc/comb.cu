@@ -13,12 +13,15 @@
 //     the symbols match or when h > v.
 //   * One warp combs one row stripe of 32*TM rows: lane l keeps rows
 //     [l*TM, l*TM+TM) of the stripe -- their symbols and h strands -- in
-//     registers for the whole stripe.  Columns advance in blocks of 4; at step
-//     t lane l combs block t-l, so the warp is a 32-deep systolic pipeline and
-//     the 4 v strands of a block travel lane to lane with __shfl_up_sync.
+//     registers for the whole stripe.  Columns advance in blocks of TW (4, or
+//     8 for short stripe chains); at step t lane l combs block t-l, so the
+//     warp is a 32-deep systolic pipeline and the v strands of a block travel
+//     lane to lane with __shfl_up_sync.  Between pipeline fill and drain the
+//     steps run without bounds checks and load their column symbols one step
+//     ahead.
 //   * Lane 31's output is the bottom edge of the stripe.  For the last stripe it
 //     is the final v; otherwise it is written to a per-pair scratch row in HBM
-//     and a progress counter is released every 8 blocks.  Lane 0 of the next
+//     and a progress counter is released every 32 columns.  Lane 0 of the next
 //     stripe (another warp, usually on another SM) acquires that counter and
 //     streams the row back with 16-byte cp.async.cg copies, 4 blocks ahead.
 //     The scratch row is reused in place: stripe s+1 overwrites block c only
@@ -26,7 +29,9 @@
 //   * Warps take stripes from a global ticket counter.  Stripes of one pair
 //     have consecutive tickets, so a stripe's producer was claimed earlier by
 //     a running warp and every wait ends; each wait is additionally bounded by
-//     %globaltimer and raises DEV_ERR_TIMEOUT instead of hanging.
+//     %globaltimer and raises DEV_ERR_TIMEOUT instead of hanging.  When all
+//     stripes fit at once, each SM runs one block of ceil(stripes / SMs)
+//     warps, so that the stripes spread evenly over the SMs.
 //   * Rows past m and columns past n are masked by data, not by branches:
 //     a masked row has symbol -1 and h = INT_MIN (never swaps), a masked column
 //     has symbol -2 and v = INT_MAX (never swaps), so edge tiles need no host
@@ -755,6 +760,7 @@ __global__ void strands_to_perm_kernel(const int32_t *__restrict__ h, int32_t m,
 // average 13.8 set the pace of the whole wavefront.)  Dynamic shared memory of
 // more than half an SM keeps a second block off every SM.
 constexpr int WF_SM_WARPS = 16;
+constexpr int MAX_DEVICES = 64;
 
 struct Balanced {
     bool ok = false;
@@ -786,16 +792,21 @@ slcs_status balanced_setup(Balanced &B)
 template <int TM, int TW>
 slcs_status launch_balanced(const CombLaunch &L, long sms, cudaStream_t stream, int *grid_out, bool *done)
 {
-    static Balanced B;
-    static int state = -1;
+    // Function attributes belong to a device: one set-up per device.
+    static Balanced per_dev[MAX_DEVICES];
+    static bool ready[MAX_DEVICES] = {};
     static std::mutex mu;
     *done = false;
+    int dev = 0;
+    SLCS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= MAX_DEVICES) return SLCS_OK; // plain persistent launch
+    Balanced &B = per_dev[dev];
     {
         std::lock_guard<std::mutex> g(mu);
-        if (state < 0) {
+        if (!ready[dev]) {
             const slcs_status s = balanced_setup<TM, TW>(B);
             if (s != SLCS_OK) return s;
-            state = 1;
+            ready[dev] = true;
         }
     }
     if (!B.ok || sms < 1) return SLCS_OK;
