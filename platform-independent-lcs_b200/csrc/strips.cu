@@ -107,31 +107,38 @@ struct Merger {
         for (int j = 0; j < par; ++j)
             if (join[j]) cudaEventDestroy(join[j]);
     }
+    // On an error the streams already forked are still joined back, so that
+    // the caller's stream does not run ahead of (and free the workspace of)
+    // products still in flight.
     slcs_status level(std::vector<Job> &jobs, int32_t *dst)
     {
         SLCS_CUDA(cudaEventRecord(fork, st));
+        slcs_status s = SLCS_OK;
+        auto cu = [&](cudaError_t e, const char *what) {
+            if (s == SLCS_OK && e != cudaSuccess) s = cuda_fail(e, what);
+        };
         int used = 0, turn = 0;
         int64_t off = 0;
         for (Job &J : jobs) {
             std::vector<Perm> &lv = *J.list;
             std::vector<Perm> out;
-            for (size_t i = 0; i < lv.size(); i += 2) {
+            for (size_t i = 0; i < lv.size() && s == SLCS_OK; i += 2) {
                 if (i + 1 < lv.size()) {
                     const int j = turn++ % par;
                     if (j >= used) {
-                        SLCS_CUDA(cudaStreamWaitEvent(side[j], fork, 0));
+                        cu(cudaStreamWaitEvent(side[j], fork, 0), "fork wait");
                         used = j + 1;
                     }
                     const int64_t size = lv[i].size + lv[i + 1].size - J.k;
-                    const slcs_status s = launch_braid(lv[i].p, int(lv[i].size), lv[i + 1].p, int(lv[i + 1].size), J.k,
-                                                       J.row_glue, dst + off, cutoff, ws + ws_bytes * size_t(j),
-                                                       ws_bytes, side[j]);
-                    if (s != SLCS_OK) return s;
+                    if (s == SLCS_OK)
+                        s = launch_braid(lv[i].p, int(lv[i].size), lv[i + 1].p, int(lv[i + 1].size), J.k,
+                                         J.row_glue, dst + off, cutoff, ws + ws_bytes * size_t(j), ws_bytes, side[j]);
                     out.push_back({dst + off, size});
                     off += size;
                 } else {
-                    SLCS_CUDA(cudaMemcpyAsync(dst + off, lv[i].p, sizeof(int32_t) * size_t(lv[i].size),
-                                              cudaMemcpyDeviceToDevice, st));
+                    cu(cudaMemcpyAsync(dst + off, lv[i].p, sizeof(int32_t) * size_t(lv[i].size),
+                                       cudaMemcpyDeviceToDevice, st),
+                       "odd part copy");
                     out.push_back({dst + off, lv[i].size});
                     off += lv[i].size;
                 }
@@ -139,10 +146,14 @@ struct Merger {
             lv.swap(out);
         }
         for (int j = 0; j < used; ++j) {
-            SLCS_CUDA(cudaEventRecord(join[j], side[j]));
-            SLCS_CUDA(cudaStreamWaitEvent(st, join[j], 0));
+            const cudaError_t e1 = cudaEventRecord(join[j], side[j]);
+            const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamWaitEvent(st, join[j], 0) : e1;
+            if (e2 != cudaSuccess) {
+                cu(e2, "join");
+                cudaStreamSynchronize(side[j]); // could not order the streams: wait here
+            }
         }
-        return SLCS_OK;
+        return s;
     }
 };
 
