@@ -10,8 +10,6 @@ import json
 import os
 import time
 
-import numpy as np
-
 from . import Config, check, lib, strands_to_permutation, permutation_hash
 
 HERE = os.path.dirname(os.path.abspath(__file__))

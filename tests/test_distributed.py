@@ -3,7 +3,6 @@ widths, the merge schedule, LPT sharding, and the send/recv merge tree of one
 long pair, with the compute steps done by the CPU oracle so that the exchange
 logic is checked without a GPU."""
 import os
-import sys
 import tempfile
 
 import numpy as np
