@@ -122,9 +122,14 @@ typedef struct {
     int32_t bands;        /* row bands of a                                          */
     int32_t braid_cutoff; /* steady-ant cutoff of the merge products (0: no merge)   */
     int32_t stripes;      /* row stripes of all tiles (warp tasks of the comb)       */
-    int32_t reserved[9];
+    int32_t cols_per_step;/* wavefront columns per step (4 or 8) for b aligned to 8  */
+    int32_t reserved[8];
 } slcs_pair_info;
 SLCS_API slcs_status slcs_pair_plan_info(int32_t m, int32_t n, const slcs_config *cfg, slcs_pair_info *info);
+/* The same plan for a device of `sms` SMs; touches no device (planning ahead
+ * for another GPU, tests of the rules on a machine without one). */
+SLCS_API slcs_status slcs_pair_plan_info_sms(int32_t m, int32_t n, const slcs_config *cfg, int32_t sms,
+                                             slcs_pair_info *info);
 
 /* One pair, device pointers, without allocating anything.  No counterpart in
  * the reference; it exists for callers that cannot allocate device memory at

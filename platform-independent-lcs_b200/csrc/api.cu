@@ -65,10 +65,10 @@ DeviceState &dev_state()
     return s;
 }
 
-int pick_tile_m(const slcs_config *cfg, int32_t m_typical, int64_t total_cells)
+// Rows per lane for pairs of about m_typical rows on a device of `sms` SMs.
+int pick_tile_m_for(const slcs_config *cfg, int32_t m_typical, int sms)
 {
     if (cfg && cfg->tile_m) return cfg->tile_m;
-    (void)total_cells;
     if (m_typical >= (1 << 19)) {
         // All stripes of one long pair are resident at once and every warp
         // stays on one SM sub-partition (4 per SM), so the busiest
@@ -76,7 +76,7 @@ int pick_tile_m(const slcs_config *cfg, int32_t m_typical, int64_t total_cells)
         // its rows, ceil(stripes / sub-partitions) * rows per stripe (2^20
         // rows: 14 -> 2341 stripes, 4 per sub-partition; 16 -> 2048 stripes,
         // still 4 on most).  Ties go to the taller stripe.
-        const int64_t parts = 4 * int64_t(std::max(1, sm_count()));
+        const int64_t parts = 4 * int64_t(std::max(1, sms));
         int best = 16;
         int64_t best_rows = INT64_MAX;
         for (int tm : {16, 14, 12}) {
@@ -95,6 +95,14 @@ int pick_tile_m(const slcs_config *cfg, int32_t m_typical, int64_t total_cells)
     if (m_typical <= 64) return 2;
     if (m_typical <= 128) return 4;
     return 8;
+}
+
+int pick_tile_m(const slcs_config *cfg, int32_t m_typical, int64_t total_cells)
+{
+    (void)total_cells;
+    // The SM count matters only to tall pairs; shorter ones need no device.
+    const bool tall = !(cfg && cfg->tile_m) && m_typical >= (1 << 19);
+    return pick_tile_m_for(cfg, m_typical, tall ? sm_count() : 1);
 }
 
 // Column strips for one pair when nothing is configured, fitted to B200
@@ -152,11 +160,11 @@ struct PairPlan {
     slcs_config c;
 };
 
-slcs_status plan_pair(int32_t m, int32_t n, const slcs_config *cfg, PairPlan *P)
+slcs_status plan_pair(int32_t m, int32_t n, const slcs_config *cfg, int sms, PairPlan *P)
 {
     P->c = cfg ? *cfg : slcs_config{};
     slcs_config &c = P->c;
-    const int tm = pick_tile_m(cfg, m, int64_t(m) * n);
+    const int tm = pick_tile_m_for(cfg, m, sms);
     if (!tile_m_supported(tm)) return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 14, 16");
     const bool auto_all = !cfg || (cfg->algo == SLCS_ALGO_AUTO && cfg->tile_m == 0 && cfg->warps == 0 &&
                                    cfg->strips == 0 && cfg->bands == 0);
@@ -447,7 +455,7 @@ slcs_status slcs_comb_pair(const uint8_t *a, int32_t m, const uint8_t *b, int32_
     if (m == 0 || n == 0) return write_identity(h_out, m, v_out, n, st);
     (void)sm_count(); // per-device set-up (memory pool) before the first allocation
     PairPlan pp;
-    const slcs_status ps = plan_pair(m, n, cfg, &pp);
+    const slcs_status ps = plan_pair(m, n, cfg, sm_count(), &pp);
     if (ps != SLCS_OK) return ps;
     const int tm = pp.c.tile_m;
     if (pp.c.algo == SLCS_ALGO_STRIPS) return comb_strips(a, m, b, n, h_out, v_out, &pp.c, tm, pp.c.warps, st);
@@ -892,24 +900,47 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
     return SLCS_OK;
 }
 
+slcs_status slcs_pair_plan_info_sms(int32_t m, int32_t n, const slcs_config *cfg, int32_t sms, slcs_pair_info *info)
+{
+    if (!info) return fail(SLCS_ERR_INVALID, "null info");
+    if (m < 0 || n < 0 || sms < 1) return fail(SLCS_ERR_INVALID, "m and n must be >= 0 and sms >= 1");
+    *info = slcs_pair_info{};
+    if (m == 0 || n == 0) return SLCS_OK;
+    PairPlan pp;
+    const slcs_status s = plan_pair(m, n, cfg, sms, &pp);
+    if (s != SLCS_OK) return s;
+    const slcs_config &c = pp.c;
+    info->algo = c.algo;
+    info->tile_m = c.tile_m;
+    info->warps = c.warps;
+    info->strips = c.strips;
+    info->bands = c.bands;
+    info->braid_cutoff = c.algo == SLCS_ALGO_STRIPS ? c.braid_cutoff : 0;
+    const int64_t stripes = stripes_of(m, c.tile_m);
+    info->stripes = int32_t(stripes * (c.algo == SLCS_ALGO_STRIPS ? c.strips : 1));
+    // Columns per step as the launch picks them for a b aligned to 8 bytes:
+    // the longest chain is the tallest band's, the narrowest tile the
+    // narrowest strip.
+    int64_t chain = stripes, width = n;
+    if (c.algo == SLCS_ALGO_STRIPS) {
+        chain = 0;
+        for (int32_t h : band_heights(m, c.bands, c.tile_m)) chain = std::max<int64_t>(chain, stripes_of(h, c.tile_m));
+        width = INT64_MAX;
+        for (int32_t w : strip_widths(n, c.strips)) width = std::min<int64_t>(width, w);
+    }
+    info->cols_per_step = pick_tw(c.tile_m, chain, width, nullptr);
+    return SLCS_OK;
+}
+
 slcs_status slcs_pair_plan_info(int32_t m, int32_t n, const slcs_config *cfg, slcs_pair_info *info)
 {
     if (!info) return fail(SLCS_ERR_INVALID, "null info");
     if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
-    *info = slcs_pair_info{};
-    if (m == 0 || n == 0) return SLCS_OK;
-    (void)sm_count();
-    PairPlan pp;
-    const slcs_status s = plan_pair(m, n, cfg, &pp);
-    if (s != SLCS_OK) return s;
-    info->algo = pp.c.algo;
-    info->tile_m = pp.c.tile_m;
-    info->warps = pp.c.warps;
-    info->strips = pp.c.strips;
-    info->bands = pp.c.bands;
-    info->braid_cutoff = pp.c.algo == SLCS_ALGO_STRIPS ? pp.c.braid_cutoff : 0;
-    info->stripes = stripes_of(m, pp.c.tile_m) * (pp.c.algo == SLCS_ALGO_STRIPS ? pp.c.strips : 1);
-    return SLCS_OK;
+    if (m == 0 || n == 0) {
+        *info = slcs_pair_info{};
+        return SLCS_OK;
+    }
+    return slcs_pair_plan_info_sms(m, n, cfg, sm_count(), info);
 }
 
 slcs_status slcs_batch_plan_info(const slcs_batch_plan *P, slcs_plan_info *info)

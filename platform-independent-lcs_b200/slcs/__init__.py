@@ -60,7 +60,7 @@ class PlanInfo(ctypes.Structure):
 class PairInfo(ctypes.Structure):
     _fields_ = [("algo", ctypes.c_int32), ("tile_m", ctypes.c_int32), ("warps", ctypes.c_int32),
                 ("strips", ctypes.c_int32), ("bands", ctypes.c_int32), ("braid_cutoff", ctypes.c_int32),
-                ("stripes", ctypes.c_int32), ("reserved", ctypes.c_int32 * 9)]
+                ("stripes", ctypes.c_int32), ("cols_per_step", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
@@ -100,6 +100,7 @@ def lib():
         L.slcs_batch_plan_launches.restype = _i32
         L.slcs_batch_plan_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
         L.slcs_pair_plan_info.argtypes = [_i32, _i32, ctypes.POINTER(Config), ctypes.POINTER(PairInfo)]
+        L.slcs_pair_plan_info_sms.argtypes = [_i32, _i32, ctypes.POINTER(Config), _i32, ctypes.POINTER(PairInfo)]
         L.slcs_strands_to_permutation.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, _vp]
         L.slcs_permutation_to_strands.argtypes = [_vp, _i32, _i32, _vp, _vp, _vp]
         L.slcs_substring_llcs.argtypes = [_vp, _i32, _i32, _vp, _vp, _i32, _vp, _vp]
@@ -155,11 +156,16 @@ def comb_pair(a, b, cfg: Optional[Config] = None, stream=None, out=None):
     return h, v
 
 
-def pair_plan_info(m: int, n: int, cfg: Optional[Config] = None) -> dict:
+def pair_plan_info(m: int, n: int, cfg: Optional[Config] = None, sms: Optional[int] = None) -> dict:
     """How comb_pair combs an m x n pair under cfg (kernel family, rows per
-    lane, warps, strips, bands, braid cutoff, stripes); launches nothing."""
+    lane, warps, strips, bands, braid cutoff, stripes, columns per step);
+    launches nothing.  With `sms`, plans for a device of that many SMs and
+    needs no device at all."""
     pi = PairInfo()
-    check(lib().slcs_pair_plan_info(int(m), int(n), _cfg(cfg), ctypes.byref(pi)))
+    if sms is None:
+        check(lib().slcs_pair_plan_info(int(m), int(n), _cfg(cfg), ctypes.byref(pi)))
+    else:
+        check(lib().slcs_pair_plan_info_sms(int(m), int(n), _cfg(cfg), int(sms), ctypes.byref(pi)))
     return pi.as_dict()
 
 
