@@ -186,6 +186,34 @@ def comb_strips(a, b, strips: int, nthreads=None):
     return c2r
 
 
+def comb_tiles(a, b, heights, widths):
+    """row_to_col of P(a, b) from tiles: a cut into row bands of the given
+    heights, b into column strips of the given widths; every tile combed
+    apart, each band's strips glued left to right by
+    staggered_multiply<false> with overlap = band height, then the bands top
+    to bottom by staggered_multiply<true> with overlap = len(b)
+    (src/braid_multiplication.hpp:273-407).  The library's tile mode merges
+    in this order (balanced trees instead of left to right chains)."""
+    a = np.ascontiguousarray(a, np.uint8)
+    b = np.ascontiguousarray(b, np.uint8)
+    assert sum(heights) == len(a) and sum(widths) == len(b)
+    band_perms = []
+    r0 = 0
+    for hgt in heights:
+        c0 = 0
+        P = None
+        for w in widths:
+            T = from_strands(*comb(a[r0:r0 + hgt], b[c0:c0 + w]))[0]
+            P = T if P is None else staggered_multiply(P, T, hgt, False)[0]
+            c0 += w
+        band_perms.append(P)
+        r0 += hgt
+    P = band_perms[0]
+    for Q in band_perms[1:]:
+        P = staggered_multiply(P, Q, len(b), True)[0]
+    return P
+
+
 # --------------------------------------------------------------------------
 # reference wrappers
 # --------------------------------------------------------------------------

@@ -117,6 +117,21 @@ def test_strip_composition_equals_direct():
         np.testing.assert_array_equal(O.comb_strips(a, b, strips, nthreads=4), direct)
 
 
+def test_tile_composition_equals_direct():
+    """Row bands x column strips, glued strips first (overlap = band height)
+    and bands second (overlap n), give P(a, b): the algebra of the library's
+    tile mode, on uneven bands and strips and with bands of one row."""
+    rng = np.random.default_rng(6)
+    for m, n, heights, widths in [(300, 200, [100, 100, 100], [50, 150]), (257, 129, [1, 128, 128], [64, 65]),
+                                  (64, 300, [64], [16, 16, 268]), (500, 1, [250, 250], [1]),
+                                  (333, 444, [32, 1, 300], [100, 44, 300])]:
+        sigma = int(rng.choice([2, 4, 20]))
+        a = rng.integers(0, sigma, m, dtype=np.uint8)
+        b = rng.integers(0, sigma, n, dtype=np.uint8)
+        direct = O.from_strands(*O.comb(a, b))[0]
+        np.testing.assert_array_equal(O.comb_tiles(a, b, heights, widths), direct)
+
+
 def test_llcs_identity():
     """LLCS = n - #{j : v[j] >= m} agrees with the classic prefix DP."""
     rng = np.random.default_rng(6)
