@@ -74,4 +74,4 @@ void Lcs_Semi_B200_With(LcsProblemContext &ctx, const B200Variant &variant)
     ctx.length_of_lcs = n - unmatched;
 }
 
-void Lcs_Semi_B200(LcsProblemContext &ctx) { Lcs_Semi_B200_With(ctx, B200Variant{0, 0, 0, 0, 0}); }
+void Lcs_Semi_B200(LcsProblemContext &ctx) { Lcs_Semi_B200_With(ctx, B200Variant{0, 0, 0, 0, 0, 0}); }
