@@ -7,9 +7,19 @@ with the plain per-pair launch loop and the 2^20 x 2^20 pair measured beside
 it, and the dominant kernel stated against the measured integer roofline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl slcs|reference]
+    python bench.py --case batch|pair|default|braid [size] [tile_m|cutoff]
 
-Under torchrun (N > 1) every rank combs its own batch (weak scaling, no
-data-path collective); the time is the maximum over ranks.
+With N > 1 (under torchrun, or launched by bench.py itself when no
+WORLD_SIZE is set) one batch of N x 20,000 pairs is dealt out over the ranks
+longest first (weak scaling: 20,000 pairs per GPU, no data-path collective);
+the time is the maximum over ranks.
+
+--case runs one small, self-contained launch for an ncu capture (one warm-up
+launch, then the launch to capture; a few hundred MB on the device at most):
+  batch [npairs] [tile_m]   the read/window batch (default 20,000 pairs)
+  pair [length] [tile_m]    one square uniform pair (default 65536)
+  default [131072|1048576]  the 131072 mutated pair (or the 2^20 pair), default rule
+  braid [k] [cutoff]        one staggered product of overlap k (default 2^18)
 """
 from __future__ import annotations
 
@@ -39,6 +49,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["slcs", "reference"], default="slcs")
     ap.add_argument("--no-extras", action="store_true", help="skip the per-pair loop and the 2^20 pair")
+    ap.add_argument("--case", nargs="+", metavar="ARG", help="one small launch for an ncu capture (see above)")
     return ap.parse_args()
 
 
@@ -118,26 +129,18 @@ def read_traffic(kernel_key: str):
 # reference arm: the reference's own CPU code (oracle/_ref) on host cores
 # ---------------------------------------------------------------------------
 def run_reference(args, batch):
+    """The reference's CPU code over the whole batch per step, all host threads."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    kind = "reference"
-    if O.ref_lib() is None:
-        kind = "port"
+    kind = "reference" if O.ref_lib() is not None else "port"
     threads = os.cpu_count() or 1
-    sample = min(batch.npairs, 4000)
-    ms = batch.ms[:sample]
-    ns = batch.ns[:sample]
-    cells = int(np.sum(ms.astype(np.int64) * ns))
-    sizes = ms.astype(np.int64) + ns
-    off = np.zeros(sample, np.int64)
-    off[1:] = np.cumsum(sizes)[:-1]
-    total = int(sizes.sum())
+    off, total = batch.strand_offsets()
     if kind == "reference":
         ab, bb = batch.a_blob.astype(np.int32), batch.b_blob.astype(np.int32)
-        step = lambda: O.ref_comb_batch(ab, bb, batch.a_off[:sample], batch.b_off[:sample], ms, ns, off, total,
+        step = lambda: O.ref_comb_batch(ab, bb, batch.a_off, batch.b_off, batch.ms, batch.ns, off, total,
                                         nthreads=threads)
     else:
-        step = lambda: O.comb_batch(batch.a_blob, batch.b_blob, batch.a_off[:sample], batch.b_off[:sample], ms, ns,
+        step = lambda: O.comb_batch(batch.a_blob, batch.b_blob, batch.a_off, batch.b_off, batch.ms, batch.ns,
                                     off, total, nthreads=threads)
     for _ in range(max(1, min(args.warmup, 2))):
         step()
@@ -145,12 +148,12 @@ def run_reference(args, batch):
     for _ in range(args.steps):
         step()
     dt = (time.perf_counter() - t0) / args.steps
-    value = cells / dt / 1e9
-    desc = f"first {sample} of the {batch.npairs} read/window pairs ({cells} cells) per step"
+    value = batch.cells / dt / 1e9
+    desc = f"all {batch.npairs} read/window pairs ({batch.cells} cells) per step"
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": "reads_20000", "pairs": batch.npairs, "sample_pairs": sample},
+            "config": {"workload": "reads_20000", "pairs": batch.npairs},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -177,9 +180,81 @@ def cpu_baseline(batch):
             "sample": f"all {batch.npairs} pairs ({batch.cells} cells), one pass, {dt:.2f} s"}, out
 
 
+def relaunch_ranks(args) -> int:
+    """--gpus N > 1 without a torchrun environment: start N ranks of this
+    script under torch.distributed.run (one process per GPU) and return the
+    launcher's exit status."""
+    import socket
+    import subprocess
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
+
+
+def run_case(case) -> int:
+    """One small launch for an ncu capture: a warm-up launch, then the launch
+    to capture, and a check of the device status word."""
+    import torch
+    import slcs
+    from slcs import workloads as W
+    kind = case[0]
+    size = int(case[1]) if len(case) > 1 else 0
+    knob = int(case[2]) if len(case) > 2 else 0
+    dev = torch.device("cuda:0")
+    if kind == "batch":
+        batch = W.reads_20000(npairs=size or 20000)
+        _, total = batch.strand_offsets()
+        plan = slcs.BatchPlan(slcs.pair_descs(batch), slcs.Config.make(tile_m=knob or None))
+        a = torch.from_numpy(batch.a_blob).to(dev)
+        b = torch.from_numpy(batch.b_blob).to(dev)
+        out = torch.empty(total, dtype=torch.int32, device=dev)
+        for _ in range(2):
+            plan.run(a, b, out)
+        torch.cuda.synchronize()
+        plan.close()
+    elif kind == "pair":
+        n = size or 65536
+        rng = np.random.default_rng(1)
+        a = torch.from_numpy(rng.integers(0, 4, n, dtype=np.uint8)).to(dev)
+        b = torch.from_numpy(rng.integers(0, 4, n, dtype=np.uint8)).to(dev)
+        out = torch.empty(2 * n, dtype=torch.int32, device=dev)
+        cfg = slcs.Config.make(tile_m=knob or None, wait_ms=600000)  # tile 0: the library's rule
+        for _ in range(2):
+            slcs.comb_pair(a, b, cfg=cfg, out=out)
+        torch.cuda.synchronize()
+    elif kind == "default":
+        a_h, b_h = W.pair_131072_mutated() if (size or 131072) == 131072 else W.pair_1m()
+        a = torch.from_numpy(a_h).to(dev)
+        b = torch.from_numpy(b_h).to(dev)
+        out = torch.empty(len(a_h) + len(b_h), dtype=torch.int32, device=dev)
+        for _ in range(2):
+            slcs.comb_pair(a, b, cfg=slcs.Config.make(wait_ms=600000), out=out)
+        torch.cuda.synchronize()
+    elif kind == "braid":
+        k = size or (1 << 18)
+        rng = np.random.default_rng(2)
+        P = torch.from_numpy(rng.permutation(k + 1000).astype(np.int32)).to(dev)
+        Q = torch.from_numpy(rng.permutation(k + 3000).astype(np.int32)).to(dev)
+        cfg = slcs.Config.make(braid_cutoff=knob or None)
+        for _ in range(2):
+            slcs.braid_multiply(P, Q, k, False, cfg=cfg)
+        torch.cuda.synchronize()
+    else:
+        print(f"unknown case {kind}", file=sys.stderr)
+        return 2
+    slcs.device_status(0)
+    print(f"case {' '.join(case)} done")
+    return 0
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_env()
+    if args.case:
+        return run_case(args.case)
     from slcs import workloads as W
     if args.impl == "reference":
         if rank != 0:
@@ -187,11 +262,20 @@ def main():
         batch = W.reads_20000()
         print(json.dumps(run_reference(args, batch)), flush=True)
         return 0
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        return relaunch_ranks(args)
+    if world != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE {world}", file=sys.stderr)
+        return 2
 
     import torch
     import slcs
+    from slcs import distributed as D
     from slcs import tuning
 
+    if not torch.cuda.is_available():
+        print("bench.py: the GPU arm needs a CUDA device", file=sys.stderr)
+        return 2
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     pg = None
@@ -200,7 +284,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
 
-    batch = W.reads_20000(seed=4 + rank)
+    # One batch of 20,000 pairs per GPU, dealt out longest first (rank 0 of a
+    # single GPU gets the whole 20,000-pair batch, whose digest is committed).
+    full = W.reads_20000(npairs=20000 * world)
+    if world > 1:
+        shard = D.shard_pairs(full.ms.astype(np.int64) * full.ns, world)[rank]
+        batch = full.subset(shard)
+    else:
+        batch = full
     descs = slcs.pair_descs(batch)
     _, total = batch.strand_offsets()
     a_d = torch.from_numpy(batch.a_blob).to(dev)
@@ -259,13 +350,14 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
-    cells_all = batch.cells * world
+    cells_all = full.cells
     value = cells_all / (ms_per_step * 1e-3) / 1e9
     kern_gcups = batch.cells / (ms_per_step * 1e-3) / 1e9
 
-    # parity of the timed output with the committed golden digest (rank 0's batch)
+    # parity of the timed output with the committed golden digest (one GPU:
+    # the batch is exactly the 20,000 pairs whose strands were digested)
     bitexact = None
-    if rank == 0:
+    if world == 1:
         import hashlib
         g = json.load(open(os.path.join(ROOT, "tests", "golden", "golden.json")))
         bitexact = hashlib.sha256(out.cpu().numpy().tobytes()).hexdigest() == g["reads_20000"]["sha256_strands"]
@@ -299,10 +391,11 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": "reads_20000", "pairs_per_gpu": batch.npairs, "cells_per_gpu_step": batch.cells,
+        "config": {"workload": "reads_20000", "pairs_per_gpu": batch.npairs, "pairs": full.npairs,
+                   "cells_per_gpu_step": batch.cells,
                    "variant": dict(plan.info, graph=bool(cfg.use_graph)),
                    "tuned_by": tuned_by, "tuning": tuning_info, "l2": "flushed between steps (256 MiB write)",
-                   "parallelism": f"{world} independent batches (weak)"},
+                   "parallelism": f"{world} shards of one batch, dealt longest first (weak)"},
         "e2e": e2e,
         "gpu_launches": args.steps * plan.launches,
         "roofline": {"bound": "int32", "achieved": kern_gcups, "peak": roof_gcups, "unit": "GCUPS",

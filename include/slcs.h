@@ -134,18 +134,21 @@ SLCS_API slcs_status slcs_pair_plan_info_sms(int32_t m, int32_t n, const slcs_co
 /* One pair, device pointers, without allocating anything.  No counterpart in
  * the reference; it exists for callers that cannot allocate device memory at
  * call time (a stream being captured into a CUDA graph with allocation
- * disallowed, a service that reserves all memory up front).  The scratch that
- * slcs_comb_pair allocates lives here in one fixed device array of
- * SLCS_NOALLOC_SCRATCH_BYTES (held by every GPU that loads the library until
- * exit); a pair needing more scratch than that (about 4 bytes per column of b
- * when a has more than 32*tile_m rows, plus 4 bytes per row stripe) is refused
- * with SLCS_ERR_RANGE.  strands_out holds h (m entries) followed by v (n).
- * The first call on a device looks up the array's address (do it before any
- * stream capture).  Every call shares the one array, so calls whose work can
+ * disallowed, a service that reserves all memory up front).  The pair is
+ * combed by the wavefront kernel with slcs_comb_pair's rows-per-lane rule
+ * (never as tiles merged by braid products, which need a workspace).  The
+ * scratch that slcs_comb_pair allocates lives here in one fixed device array
+ * of SLCS_NOALLOC_SCRATCH_BYTES (held by every GPU that loads the library
+ * until exit); a pair needing more scratch than that (about 4 bytes per
+ * column of b when a has more than 32*tile_m rows, plus 4 bytes per row
+ * stripe) is refused with SLCS_ERR_RANGE before any pointer or device is
+ * touched.  strands_out holds h (m entries) followed by v (n).  The first
+ * call on a device looks up the array's address (do it before any stream
+ * capture).  Every call shares the one array, so calls whose work can
  * overlap on the GPU (different streams, or before the previous call's kernel
  * finished on another stream) race; serialise them.  Device-side wait
- * timeouts raise slcs_device_status() only if an earlier call on this device
- * created the status word. */
+ * timeouts go to a status word of this entry point, which
+ * slcs_device_status() reads (and clears) together with the others. */
 #define SLCS_NOALLOC_SCRATCH_BYTES (16u << 20)
 SLCS_API slcs_status slcs_comb_pair_noalloc(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n,
                                             int32_t *strands_out, const slcs_config *cfg, void *stream);
@@ -155,6 +158,25 @@ SLCS_API slcs_status slcs_comb_pair_noalloc(const uint8_t *a, int32_t m, const u
  * binds. */
 SLCS_API slcs_status slcs_comb_pair_host(const uint8_t *a, int32_t m, const uint8_t *b, int32_t n,
                                 int32_t *h_out, int32_t *v_out, const slcs_config *cfg);
+
+/* The reference's Word symbols (int32, src/lcs_interface_internal.hpp:16-35)
+ * as bytes, on the device: the preparation its solvers do on the host
+ * (src/lcs_grid.hpp:168-208, 433-449) moved next to the comb.  Only equality
+ * of symbols matters (src/lcs_residual_fixup.hpp:49-54): symbols that all lie
+ * in 0..255 are kept, otherwise each becomes its rank among the distinct
+ * symbols of a and b.  a, b, a_out, b_out and alphabet_out are device
+ * pointers; *alphabet_out receives the number of distinct symbols, or -1 when
+ * there are more than 256 (the bytes are then all 0). */
+SLCS_API slcs_status slcs_symbols_to_bytes(const int32_t *a, int32_t m, const int32_t *b, int32_t n, uint8_t *a_out,
+                                           uint8_t *b_out, int32_t *alphabet_out, void *stream);
+
+/* One pair of Word symbols from host memory: copies the words in, maps them
+ * to bytes on the device (slcs_symbols_to_bytes), combs, copies the strands
+ * out and synchronises.  More than 256 distinct symbols give SLCS_ERR_RANGE
+ * before any comb.  The entry point the reference-side procedure adapter
+ * binds (src/algorithm_registry.cpp:59-73 hands it the Word arrays). */
+SLCS_API slcs_status slcs_comb_pair_words_host(const int32_t *a, int32_t m, const int32_t *b, int32_t n,
+                                               int32_t *h_out, int32_t *v_out, const slcs_config *cfg);
 
 /* Many independent pairs in one persistent launch with a device work queue.
  * pairs: host array of npairs descriptors; blobs/out: device pointers.
@@ -271,6 +293,14 @@ SLCS_API slcs_status slcs_costmodel_grad(const float *params, int32_t k, const f
  * of the combing rule on register-resident strands (cells/s). */
 SLCS_API slcs_status slcs_probe_int_rates(int32_t iters, double *int32_ops_per_s, double *cells_per_s,
                                           void *stream);
+
+/* Check of the failure path the reference reports through exceptions
+ * (src/main.cpp:83-94): enqueues one wavefront launch of a small two-stripe
+ * pair whose first stripe is never claimed, so the second stripe's bounded
+ * wait for it runs out after wait_ms (1..5000).  After synchronising the
+ * stream, slcs_device_status() reports SLCS_ERR_TIMEOUT; the context stays
+ * usable and later calls run normally. */
+SLCS_API slcs_status slcs_probe_wait_expiry(int32_t wait_ms, void *stream);
 
 #ifdef __cplusplus
 }

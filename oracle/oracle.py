@@ -34,9 +34,14 @@ def _ptr(arr, ty):
     return arr.ctypes.data_as(ty)
 
 
-def build():
-    """Compile the oracle (and the reference bridge when its sources exist)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+def build(ref_src: str | None = None):
+    """Compile the oracle; with ``ref_src`` (the reference's ``src/``
+    directory, else the ``SLCS_REF_SRC`` environment variable) also the
+    reference bridge."""
+    ref_src = ref_src or os.environ.get("SLCS_REF_SRC")
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if ref_src:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={ref_src}"], check=True)
 
 
 def lib():
@@ -73,7 +78,7 @@ def ref_lib():
     if _REF is None:
         path = os.path.join(HERE, "_ref", "libslcs_ref.so")
         if not os.path.exists(path):
-            if os.path.isdir("/root/reference/src"):
+            if os.environ.get("SLCS_REF_SRC"):
                 build()
             if not os.path.exists(path):
                 return None

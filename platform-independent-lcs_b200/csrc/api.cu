@@ -65,6 +65,8 @@ DeviceState &dev_state()
     return s;
 }
 
+} // namespace
+
 // Rows per lane for pairs of about m_typical rows on a device of `sms` SMs.
 int pick_tile_m_for(const slcs_config *cfg, int32_t m_typical, int sms)
 {
@@ -96,6 +98,8 @@ int pick_tile_m_for(const slcs_config *cfg, int32_t m_typical, int sms)
     if (m_typical <= 128) return 4;
     return 8;
 }
+
+namespace {
 
 int pick_tile_m(const slcs_config *cfg, int32_t m_typical, int64_t total_cells)
 {
@@ -151,8 +155,12 @@ int auto_bands(int32_t m, int32_t n, int tm)
     return best;
 }
 
+} // namespace
+
 // 14 or 16 rows per lane leave room for 8 warps per block; the smaller tiles run 4.
 int pick_warps(const slcs_config *cfg, int tm) { return (cfg && cfg->warps) ? cfg->warps : (tm >= 14 ? 8 : 4); }
+
+namespace {
 
 // How slcs_comb_pair combs one pair: the effective configuration (algo
 // WAVEFRONT or STRIPS with tile_m, warps, strips, bands, braid_cutoff set).
@@ -437,6 +445,7 @@ slcs_status slcs_device_status(int32_t device, int32_t clear)
     DeviceState &s = dev_state();
     uint32_t bits = s.host_status ? __atomic_load_n(s.host_status, __ATOMIC_SEQ_CST) : 0;
     if (clear && s.host_status) __atomic_store_n(s.host_status, 0u, __ATOMIC_SEQ_CST);
+    bits |= noalloc_status_bits(clear != 0);
     if (device != cur) cudaSetDevice(cur);
     if (bits & DEV_ERR_TIMEOUT) return fail(SLCS_ERR_TIMEOUT, "a device-side wait timed out");
     if (bits & DEV_ERR_INPUT) return fail(SLCS_ERR_INVALID, "a device-side input check failed (not a permutation)");
@@ -538,6 +547,73 @@ slcs_status slcs_comb_pair_host(const uint8_t *a, int32_t m, const uint8_t *b, i
     cudaStreamDestroy(st);
     if (s != SLCS_OK) return s;
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamSynchronize");
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return slcs_device_status(dev, 1);
+}
+
+slcs_status slcs_symbols_to_bytes(const int32_t *a, int32_t m, const int32_t *b, int32_t n, uint8_t *a_out,
+                                  uint8_t *b_out, int32_t *alphabet_out, void *stream)
+{
+    if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
+    if ((m > 0 && (!a || !a_out)) || (n > 0 && (!b || !b_out)) || !alphabet_out)
+        return fail(SLCS_ERR_INVALID, "null symbol or output pointer");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    (void)sm_count(); // per-device set-up (memory pool) before the first allocation
+    void *ws = nullptr;
+    SLCS_CUDA(cudaMallocAsync(&ws, symbols_workspace_bytes(), st));
+    const slcs_status s = symbols_to_bytes(a, m, b, n, a_out, b_out, alphabet_out, ws, st);
+    SLCS_CUDA(cudaFreeAsync(ws, st));
+    return s;
+}
+
+slcs_status slcs_comb_pair_words_host(const int32_t *a, int32_t m, const int32_t *b, int32_t n, int32_t *h_out,
+                                      int32_t *v_out, const slcs_config *cfg)
+{
+    if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
+    if ((m > 0 && (!a || !h_out)) || (n > 0 && (!b || !v_out)))
+        return fail(SLCS_ERR_INVALID, "null pointer for a non-empty side");
+    if (int64_t(m) + n > INT32_MAX) return fail(SLCS_ERR_RANGE, "m+n exceeds int32 strand ids");
+    cudaStream_t st = nullptr;
+    SLCS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    // [a words | b words | a bytes | b bytes | strands | alphabet | symbol workspace]
+    const size_t o_bw = align_up(sizeof(int32_t) * size_t(m), 256);
+    const size_t o_ab = o_bw + align_up(sizeof(int32_t) * size_t(n), 256);
+    const size_t o_bb = o_ab + align_up(size_t(m) + 16, 256);
+    const size_t o_out = o_bb + align_up(size_t(n) + 16, 256);
+    const size_t o_alpha = o_out + align_up(sizeof(int32_t) * (size_t(m) + n), 256);
+    const size_t o_ws = o_alpha + 256;
+    const size_t bytes = o_ws + symbols_workspace_bytes();
+    char *buf = nullptr;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&buf), bytes, st);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(st);
+        return cuda_fail(e, "cudaMallocAsync");
+    }
+    int32_t *da = reinterpret_cast<int32_t *>(buf), *db = reinterpret_cast<int32_t *>(buf + o_bw);
+    uint8_t *ab = reinterpret_cast<uint8_t *>(buf + o_ab), *bb = reinterpret_cast<uint8_t *>(buf + o_bb);
+    int32_t *dout = reinterpret_cast<int32_t *>(buf + o_out), *dalpha = reinterpret_cast<int32_t *>(buf + o_alpha);
+    slcs_status s = SLCS_OK;
+    int32_t alphabet = 0;
+    if (m) e = cudaMemcpyAsync(da, a, sizeof(int32_t) * size_t(m), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && n) e = cudaMemcpyAsync(db, b, sizeof(int32_t) * size_t(n), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) s = symbols_to_bytes(da, m, db, n, ab, bb, dalpha, buf + o_ws, st);
+    if (e == cudaSuccess && s == SLCS_OK) e = cudaMemcpyAsync(&alphabet, dalpha, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && s == SLCS_OK) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && s == SLCS_OK && alphabet < 0)
+        s = fail(SLCS_ERR_RANGE, "more than 256 distinct symbols in a and b");
+    if (e == cudaSuccess && s == SLCS_OK) {
+        s = slcs_comb_pair(ab, m, bb, n, dout, dout + m, cfg, st);
+        if (s == SLCS_OK && m) e = cudaMemcpyAsync(h_out, dout, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, st);
+        if (s == SLCS_OK && e == cudaSuccess && n)
+            e = cudaMemcpyAsync(v_out, dout + m, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st);
+    }
+    cudaFreeAsync(buf, st);
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (s != SLCS_OK) return s;
+    if (e != cudaSuccess) return cuda_fail(e, "symbol or strand copies");
     if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamSynchronize");
     int dev = 0;
     cudaGetDevice(&dev);

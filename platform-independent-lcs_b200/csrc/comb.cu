@@ -821,23 +821,46 @@ slcs_status launch_balanced(const CombLaunch &L, long sms, cudaStream_t stream, 
     return SLCS_OK;
 }
 
-template <int TM, int WARPS, int TW>
-slcs_status launch_variant_tw(const CombLaunch &L, cudaStream_t stream, int *grid_out)
+// Resident blocks per SM of one kernel on the current device (queried once
+// per kernel and device: occupancy belongs to a device, like function
+// attributes).  The kernel is a template argument, so that every kernel
+// keeps its own table.
+template <auto Kernel>
+slcs_status occupancy_of(int threads, int *occ_out)
 {
-    const long sms = sm_count();
+    static int per_dev[MAX_DEVICES] = {}; // 0: not queried yet
+    static std::mutex mu;
+    int dev = 0;
+    SLCS_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(mu);
+    int *slot = (dev >= 0 && dev < MAX_DEVICES) ? &per_dev[dev] : nullptr;
+    if (!slot || *slot == 0) {
+        int occ = 0;
+        SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, Kernel, threads, 0));
+        if (occ < 1) occ = 1;
+        if (!slot) {
+            *occ_out = occ;
+            return SLCS_OK;
+        }
+        *slot = occ;
+    }
+    *occ_out = *slot;
+    return SLCS_OK;
+}
+
+// `sms` is the SM count of the current device (passed in by the caller, so
+// that entry points that must not allocate never touch the lazily created
+// per-device state behind sm_count()).
+template <int TM, int WARPS, int TW>
+slcs_status launch_variant_tw(const CombLaunch &L, long sms, cudaStream_t stream, int *grid_out)
+{
+    if (sms < 1) sms = 1;
     bool done = false;
     const slcs_status bs = launch_balanced<TM, TW>(L, sms, stream, grid_out, &done);
     if (bs != SLCS_OK || done) return bs;
-    static int occ = -1;
-    static std::mutex mu;
-    {
-        std::lock_guard<std::mutex> g(mu);
-        if (occ < 0) {
-            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WARPS, TW>,
-                                                                    WARPS * 32, 0));
-            if (occ < 1) occ = 1;
-        }
-    }
+    int occ = 1;
+    const slcs_status os = occupancy_of<comb_wavefront_kernel<TM, WARPS, TW>>(WARPS * 32, &occ);
+    if (os != SLCS_OK) return os;
     if (stream == PREPARE_ONLY) return SLCS_OK;
     // More stripes than fit at once: persistent blocks take stripes from the
     // ticket counter.  Beyond one block per SM the grid is rounded up to a
@@ -855,26 +878,20 @@ slcs_status launch_variant_tw(const CombLaunch &L, cudaStream_t stream, int *gri
 }
 
 template <int TM, int WARPS>
-slcs_status launch_variant(const CombLaunch &L, cudaStream_t stream, int *grid_out)
+slcs_status launch_variant(const CombLaunch &L, long sms, cudaStream_t stream, int *grid_out)
 {
     if constexpr (TM == 14 || TM == 16) {
-        if (L.tw == 8) return launch_variant_tw<TM, WARPS, 8>(L, stream, grid_out);
+        if (L.tw == 8) return launch_variant_tw<TM, WARPS, 8>(L, sms, stream, grid_out);
     }
-    return launch_variant_tw<TM, WARPS, 4>(L, stream, grid_out);
+    return launch_variant_tw<TM, WARPS, 4>(L, sms, stream, grid_out);
 }
 
 template <int TNS, int WARPS>
 slcs_status launch_batch_variant(const BatchLaunch &B, cudaStream_t stream, int *grid_out)
 {
-    static int occ = -1;
-    static std::mutex mu;
-    {
-        std::lock_guard<std::mutex> g(mu);
-        if (occ < 0) {
-            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_batch_kernel<TNS, WARPS>, WARPS * 32, 0));
-            if (occ < 1) occ = 1;
-        }
-    }
+    int occ = 1;
+    const slcs_status os = occupancy_of<comb_batch_kernel<TNS, WARPS>>(WARPS * 32, &occ);
+    if (os != SLCS_OK) return os;
     if (stream == PREPARE_ONLY) {
         if (grid_out) *grid_out = sm_count() * occ;
         return SLCS_OK;
@@ -887,55 +904,34 @@ slcs_status launch_batch_variant(const BatchLaunch &B, cudaStream_t stream, int 
     return SLCS_OK;
 }
 
-// The wavefront launch with the SM count given by the caller (used by the
-// entry point that must not allocate, so it cannot touch the lazily created
-// per-device state behind sm_count()).
-template <int TM, int WARPS>
-slcs_status launch_variant_on(const CombLaunch &L, int sms, cudaStream_t stream)
-{
-    bool done = false;
-    const slcs_status bs = launch_balanced<TM, 4>(L, sms, stream, nullptr, &done);
-    if (bs != SLCS_OK || done) return bs;
-    static int occ = -1;
-    static std::mutex mu;
-    {
-        std::lock_guard<std::mutex> g(mu);
-        if (occ < 0) {
-            SLCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, comb_wavefront_kernel<TM, WARPS, 4>,
-                                                                    WARPS * 32, 0));
-            if (occ < 1) occ = 1;
-        }
-    }
-    const long want = (long(L.ntasks) + WARPS - 1) / WARPS;
-    long grid = long(sms > 0 ? sms : 1) * occ;
-    if (want < grid) grid = want;
-    if (grid < 1) grid = 1;
-    comb_wavefront_kernel<TM, WARPS, 4><<<int(grid), WARPS * 32, 0, stream>>>(L);
-    SLCS_CUDA(cudaGetLastError());
-    return SLCS_OK;
-}
-
 } // namespace
 
-slcs_status launch_comb_on(const CombLaunch &L, int tile_m, int warps, int sms, cudaStream_t stream)
+// Dispatch on rows per lane and warps per block.
+static slcs_status launch_comb_sms(const CombLaunch &L, int tile_m, int warps, long sms, cudaStream_t stream,
+                                   int *grid_out)
 {
     if (L.ntasks <= 0) return SLCS_OK;
-#define SLCS_TM_ON(TM)                                                                     \
+#define SLCS_TM_CASE(TM)                                                                   \
     case TM:                                                                               \
-        if (warps == 2) return launch_variant_on<TM, 2>(L, sms, stream);                   \
-        if (warps == 8) return launch_variant_on<TM, 8>(L, sms, stream);                   \
-        return launch_variant_on<TM, 4>(L, sms, stream);
+        if (warps == 2) return launch_variant<TM, 2>(L, sms, stream, grid_out);            \
+        if (warps == 8) return launch_variant<TM, 8>(L, sms, stream, grid_out);            \
+        return launch_variant<TM, 4>(L, sms, stream, grid_out);
     switch (tile_m) {
-        SLCS_TM_ON(2)
-        SLCS_TM_ON(4)
-        SLCS_TM_ON(8)
-        SLCS_TM_ON(12)
-        SLCS_TM_ON(14)
-        SLCS_TM_ON(16)
+        SLCS_TM_CASE(2)
+        SLCS_TM_CASE(4)
+        SLCS_TM_CASE(8)
+        SLCS_TM_CASE(12)
+        SLCS_TM_CASE(14)
+        SLCS_TM_CASE(16)
     default:
         return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 14, 16");
     }
-#undef SLCS_TM_ON
+#undef SLCS_TM_CASE
+}
+
+slcs_status launch_comb_on(const CombLaunch &L, int tile_m, int warps, int sms, cudaStream_t stream)
+{
+    return launch_comb_sms(L, tile_m, warps, sms, stream, nullptr);
 }
 
 bool packed16_supported(int tm, int seg) { return (tm == 4 || tm == 8 || tm == 12 || tm == 16) && seg == 16; }
@@ -959,22 +955,7 @@ int rows_per_stripe(int tm) { return 32 * tm; }
 slcs_status launch_comb(const CombLaunch &L, int tile_m, int warps, cudaStream_t stream, int *grid_out)
 {
     if (L.ntasks <= 0) return SLCS_OK;
-#define SLCS_TM_CASE(TM)                                                                   \
-    case TM:                                                                               \
-        if (warps == 2) return launch_variant<TM, 2>(L, stream, grid_out);                 \
-        if (warps == 8) return launch_variant<TM, 8>(L, stream, grid_out);                 \
-        return launch_variant<TM, 4>(L, stream, grid_out);
-    switch (tile_m) {
-        SLCS_TM_CASE(2)
-        SLCS_TM_CASE(4)
-        SLCS_TM_CASE(8)
-        SLCS_TM_CASE(12)
-        SLCS_TM_CASE(14)
-        SLCS_TM_CASE(16)
-    default:
-        return fail(SLCS_ERR_UNSUPPORTED, "tile_m must be one of 2, 4, 8, 12, 14, 16");
-    }
-#undef SLCS_TM_CASE
+    return launch_comb_sms(L, tile_m, warps, sm_count(), stream, grid_out);
 }
 
 slcs_status launch_strands_to_perm(const int32_t *h, int32_t m, const int32_t *v, int32_t n, int32_t *r2c,

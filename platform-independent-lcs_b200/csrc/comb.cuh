@@ -61,6 +61,12 @@ constexpr int PACKED16_CODE = 10000;
 constexpr int PACKED16_MAX_IDS = 32767;
 bool packed16_supported(int tm, int seg);
 
+// Rows per lane that slcs_comb_pair uses for an m-row pair on a device of
+// `sms` SMs (the SM count matters only from 2^19 rows), and its warps per
+// block; cfg fields that are set win.
+int pick_tile_m_for(const slcs_config *cfg, int32_t m, int sms);
+int pick_warps(const slcs_config *cfg, int tm);
+
 // Rows of a one lane keeps in registers; supported values.
 bool tile_m_supported(int tm);
 int rows_per_stripe(int tm);

@@ -7,7 +7,11 @@
 //     stated in;
 //   * cell_rate: the seaweed cell rule itself on register-resident strands with
 //     no memory traffic at all -- the practical ceiling of any combing kernel.
-#include "slcs_internal.cuh"
+//
+// slcs_probe_wait_expiry checks the failure path of the bounded waits on the
+// device: a stripe waits for a producer that never runs, the wait runs out,
+// and the launch ends with an error status instead of a hang.
+#include "comb.cuh"
 
 namespace slcs {
 namespace {
@@ -111,4 +115,36 @@ extern "C" SLCS_API slcs_status slcs_probe_int_rates(int32_t iters, double *int3
     cudaEventDestroy(e1);
     SLCS_CUDA(cudaFreeAsync(sink, st));
     return SLCS_OK;
+}
+
+extern "C" SLCS_API slcs_status slcs_probe_wait_expiry(int32_t wait_ms, void *stream)
+{
+    if (wait_ms < 1 || wait_ms > 5000) return fail(SLCS_ERR_RANGE, "wait_ms must be in 1..5000");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // A pair of two row stripes (tile_m 2: 64 rows each) and 64 columns.
+    constexpr int TM = 2, M = 128, N = 64;
+    const size_t o_b = 256, o_out = 512, o_work = o_out + 256 * sizeof(int32_t), o_scr = o_work + 256;
+    const size_t bytes = o_scr + sizeof(int32_t) * size_t(scratch_elems(M, N, TM)) + 256;
+    char *ws = nullptr;
+    (void)sm_count(); // per-device set-up (memory pool, status word) before the allocation
+    SLCS_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&ws), bytes, st));
+    SLCS_CUDA(cudaMemsetAsync(ws, 0, bytes, st));
+    // Ticket counter preset to 1: task 0 (stripe 0, the producer) is never
+    // claimed, so nothing ever publishes the progress that stripe 1 waits for.
+    SLCS_CUDA(cudaMemsetAsync(ws + o_work, 1, 1, st));
+    CombLaunch L{};
+    L.ntasks = stripes_of(M, TM);
+    L.a_blob = reinterpret_cast<const uint8_t *>(ws);
+    L.b_blob = reinterpret_cast<const uint8_t *>(ws + o_b);
+    L.out = reinterpret_cast<int32_t *>(ws + o_out);
+    L.scratch = reinterpret_cast<int32_t *>(ws + o_scr);
+    L.counters = reinterpret_cast<int32_t *>(ws + o_work);
+    L.progress = L.counters + 4;
+    L.status = device_status_word();
+    L.wait_ns = uint64_t(wait_ms) * 1000000ull;
+    L.single.m = M;
+    L.single.n = N;
+    const slcs_status s = launch_comb(L, TM, 4, st, nullptr);
+    SLCS_CUDA(cudaFreeAsync(ws, st));
+    return s;
 }

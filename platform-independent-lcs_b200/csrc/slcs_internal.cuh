@@ -52,6 +52,15 @@ uint32_t *device_status_word();
 // The same word if an earlier call already created it, else null (never allocates).
 uint32_t *device_status_word_if_ready();
 int sm_count();
+// Error bits raised by slcs_comb_pair_noalloc kernels on the current device
+// (its own status word; 0 when it never ran there), optionally cleared.
+uint32_t noalloc_status_bits(bool clear);
+
+// Word symbols (int32) of a and b -> bytes on the device (symbols.cu); the
+// alphabet size (or -1 above 256) is written to *alphabet_out (device).
+slcs_status symbols_to_bytes(const int32_t *a, int32_t m, const int32_t *b, int32_t n, uint8_t *a_out,
+                             uint8_t *b_out, int32_t *alphabet_out, void *ws, cudaStream_t st);
+size_t symbols_workspace_bytes();
 
 // ---- device helpers ---------------------------------------------------------
 __device__ __forceinline__ uint64_t globaltimer_ns()

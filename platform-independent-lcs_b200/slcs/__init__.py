@@ -16,6 +16,7 @@ import numpy as np
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 ROOT_DIR = os.path.dirname(PKG_DIR)
 LIB_PATH = os.path.join(ROOT_DIR, "lib", "libslcs.so")
+HOST_LIB_PATH = os.path.join(ROOT_DIR, "lib", "libslcs_host.so")
 
 ALGO_AUTO, ALGO_WAVEFRONT, ALGO_STRIPS = 0, 1, 2
 
@@ -108,6 +109,10 @@ def lib():
         L.slcs_permutation_hash.restype = _i64
         L.slcs_probe_int_rates.argtypes = [_i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _vp]
         L.slcs_braid_multiply.argtypes = [_vp, _i32, _vp, _i32, _i32, _i32, _vp, ctypes.POINTER(Config), _vp]
+        L.slcs_probe_wait_expiry.argtypes = [_i32, _vp]
+        L.slcs_symbols_to_bytes.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, _vp, _vp]
+        L.slcs_comb_pair_words_host.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, ctypes.POINTER(Config)]
+        L.slcs_comb_pair_noalloc.argtypes = [_vp, _i32, _vp, _i32, _vp, ctypes.POINTER(Config), _vp]
         _LIB = L
     return _LIB
 
@@ -178,6 +183,65 @@ def comb_pair_host(a: np.ndarray, b: np.ndarray, cfg: Optional[Config] = None):
     check(lib().slcs_comb_pair_host(a.ctypes.data, len(a), b.ctypes.data, len(b), h.ctypes.data,
                                     v.ctypes.data, _cfg(cfg)))
     return h, v
+
+
+def comb_pair_words_host(a: np.ndarray, b: np.ndarray, cfg: Optional[Config] = None):
+    """Strands of one pair of Word symbols (any int32 values, at most 256
+    distinct) from host numpy arrays; the symbols become bytes on the device."""
+    a = np.ascontiguousarray(a, np.int32)
+    b = np.ascontiguousarray(b, np.int32)
+    h = np.empty(len(a), np.int32)
+    v = np.empty(len(b), np.int32)
+    check(lib().slcs_comb_pair_words_host(a.ctypes.data, len(a), b.ctypes.data, len(b), h.ctypes.data,
+                                          v.ctypes.data, _cfg(cfg)))
+    return h, v
+
+
+def symbols_to_bytes(a, b, stream=None):
+    """(a_bytes, b_bytes, alphabet) of int32 CUDA tensors of Word symbols;
+    alphabet is the number of distinct symbols, or -1 above 256."""
+    import torch
+    m, n = int(a.numel()), int(b.numel())
+    ab = torch.empty(m, dtype=torch.uint8, device=a.device)
+    bb = torch.empty(n, dtype=torch.uint8, device=a.device)
+    alpha = torch.empty(1, dtype=torch.int32, device=a.device)
+    check(lib().slcs_symbols_to_bytes(_dptr(a), m, _dptr(b), n, _dptr(ab), _dptr(bb), alpha.data_ptr(),
+                                      _stream(stream)))
+    return ab, bb, int(alpha.item())
+
+
+_HOST = None
+
+
+def host_lib():
+    """libslcs_host.so: the C++ mirror of the reference interface."""
+    global _HOST
+    if _HOST is None:
+        lib()
+        if not os.path.exists(HOST_LIB_PATH):
+            raise RuntimeError(f"libslcs_host.so not found at {HOST_LIB_PATH}")
+        H = ctypes.CDLL(HOST_LIB_PATH)
+        H.slcs_host_run_procedure.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _vp, _i32, _vp, _i32, _vp, _vp,
+                                              _vp, _vp, ctypes.c_char_p, _i32]
+        H.slcs_host_run_procedure.restype = _i32
+        _HOST = H
+    return _HOST
+
+
+def run_procedure(name: str, a: np.ndarray, b: np.ndarray, device_type: str = "gpu"):
+    """Run a registered procedure through the C++ mirror of the reference's
+    registry: (status, h, v, length_of_lcs, hash, message)."""
+    a = np.ascontiguousarray(a, np.int32)
+    b = np.ascontiguousarray(b, np.int32)
+    h = np.empty(len(a), np.int32)
+    v = np.empty(len(b), np.int32)
+    llcs = ctypes.c_int32(-1)
+    hv = ctypes.c_int64(0)
+    err = ctypes.create_string_buffer(512)
+    rc = host_lib().slcs_host_run_procedure(name.encode(), device_type.encode(), a.ctypes.data, len(a),
+                                            b.ctypes.data, len(b), h.ctypes.data, v.ctypes.data,
+                                            ctypes.addressof(llcs), ctypes.addressof(hv), err, len(err))
+    return int(rc), h, v, int(llcs.value), int(hv.value), err.value.decode(errors="replace")
 
 
 def pair_descs(batch) -> np.ndarray:
@@ -304,3 +368,9 @@ def probe_int_rates(iters: int = 4096, stream=None):
     cells = ctypes.c_double()
     check(lib().slcs_probe_int_rates(int(iters), ctypes.byref(ops), ctypes.byref(cells), _stream(stream)))
     return ops.value, cells.value
+
+
+def probe_wait_expiry(wait_ms: int = 200, stream=None):
+    """Enqueue the bounded-wait check (a stripe whose producer never runs);
+    after a synchronise, device_status() raises SlcsError with status 4."""
+    check(lib().slcs_probe_wait_expiry(int(wait_ms), _stream(stream)))

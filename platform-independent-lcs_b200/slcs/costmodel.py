@@ -22,6 +22,7 @@ from . import Config, check, lib
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 MODEL_PATH = os.path.join(HERE, "data", "costmodel.json")
+DB_PATH = os.path.join(HERE, "data", "timings.npz")
 
 # The variants the autotuner times and the model ranks.  Variant 0 is what the
 # library does when nothing is configured (the fixed heuristic).

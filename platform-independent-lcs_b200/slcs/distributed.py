@@ -25,8 +25,11 @@ of 448 rows (14 rows per lane, the library's choice for the tallest pairs).
 Any heights and widths give the same strands.
 
 The compute steps go through a kernels object (CudaKernels: the library's C
-ABI).  The exchange logic does not depend on what computes, which is how it
-is tested on CPU processes with the gloo backend.
+ABI) and the exchange through a communicator (TorchComm: torch.distributed
+point-to-point on a process group).  The exchange logic depends on neither,
+which is how it is tested on CPU processes with the gloo backend and, with
+in-process ranks that hand tensors over by device copies, through the CUDA
+kernels on one GPU.
 """
 from __future__ import annotations
 
@@ -115,17 +118,36 @@ class CudaKernels:
         return torch.empty(int(size), dtype=torch.int32, device=like.device)
 
 
-def comb_pair_distributed(a, b, group=None, kernels=None, split: str = "auto"):
+class TorchComm:
+    """Point-to-point exchange over a torch.distributed process group (NCCL
+    between GPUs, gloo between CPU processes)."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+
+    def send(self, t, dst: int):
+        import torch.distributed as dist
+        dist.send(t, group=self.group, group_dst=dst)
+
+    def recv(self, t, src: int):
+        import torch.distributed as dist
+        dist.recv(t, group=self.group, group_src=src)
+
+
+def comb_pair_distributed(a, b, group=None, kernels=None, split: str = "auto", comm=None):
     """Strands (h, v) of one pair on rank 0 (None on the other ranks).
 
     a and b are the whole strings on every rank (uint8 tensors on this rank's
     device); each rank reads only its band of a or strip of b.  split is
     "bands", "strips" or "auto" (bands when m >= n).  Every rank takes the
-    same send/recv steps in the same order."""
-    import torch.distributed as dist
+    same send/recv steps in the same order.  `comm` (rank, world, send,
+    recv) defaults to TorchComm(group)."""
     K = kernels or CudaKernels()
-    rank = dist.get_rank(group)
-    world = dist.get_world_size(group)
+    C = comm or TorchComm(group)
+    rank, world = C.rank, C.world
     m, n = int(a.numel()), int(b.numel())
     if split == "auto":
         split = "bands" if m >= n else "strips"
@@ -144,10 +166,10 @@ def comb_pair_distributed(a, b, group=None, kernels=None, split: str = "auto"):
     for rnd in merge_rounds(world):
         for dst, src in rnd:
             if rank == src:
-                dist.send(P, group=group, group_dst=dst)
+                C.send(P, dst)
             elif rank == dst:
                 Q = K.empty(sizes[src], P)
-                dist.recv(Q, group=group, group_src=src)
+                C.recv(Q, src)
                 P = K.braid(P, Q, k, rows)
         for dst, src in rnd:
             sizes[dst] = sizes[dst] + sizes[src] - k

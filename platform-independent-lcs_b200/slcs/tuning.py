@@ -49,7 +49,9 @@ def choose_batch_config(batch, timer=None, top: int = 3):
 
 
 def per_pair_loop(batch, a_d, b_d, out, stream_handle, limit=None):
-    """The plain path: one slcs_comb_pair launch per pair, device pointers."""
+    """The plain path as a caller would write it: one slcs_comb_pair call per
+    pair, device pointers (each call plans, allocates its scratch, launches
+    and frees)."""
     L = lib()
     A, B, O_ = a_d.data_ptr(), b_d.data_ptr(), out.data_ptr()
     from . import pair_descs
@@ -62,26 +64,119 @@ def per_pair_loop(batch, a_d, b_d, out, stream_handle, limit=None):
                                stream_handle))
 
 
-def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev, sampler=None):
-    """Plain per-pair loop, the 2^20 pair (best of 5 runs, with the SM clocks
-    sampled while it runs when `sampler` -- a context-manager factory with a
-    summary() -- is given), strips and braid products."""
+def per_pair_loop_lean(batch, a_d, b_d, out, stream_handle, limit=None):
+    """The plain path at its leanest: one wavefront launch per pair on
+    preallocated scratch (slcs_comb_pair_noalloc: a counter reset and the
+    kernel, nothing planned or allocated per pair)."""
+    L = lib()
+    A, B, O_ = a_d.data_ptr(), b_d.data_ptr(), out.data_ptr()
+    from . import pair_descs
+    d = pair_descs(batch)
+    n = batch.npairs if limit is None else min(limit, batch.npairs)
+    f = L.slcs_comb_pair_noalloc
+    for p in range(n):
+        m, nn = int(d["m"][p]), int(d["n"][p])
+        check(f(A + int(d["a_offset"][p]), m, B + int(d["b_offset"][p]), nn, O_ + 4 * int(d["out_offset"][p]),
+                None, stream_handle))
+
+
+def _golden():
+    try:
+        with open(os.path.join(HERE, "..", "..", "tests", "golden", "golden.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def _time_loop(loop, batch, a_d, b_d, out, st):
     import torch
-    res = {}
-    st = torch.cuda.current_stream()
-    # plain per-pair launch loop over the same batch
-    per_pair_loop(batch, a_d, b_d, out, st.cuda_stream, limit=200)
+    loop(batch, a_d, b_d, out, st.cuda_stream, limit=200)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     e0.record(st)
-    per_pair_loop(batch, a_d, b_d, out, st.cuda_stream)
+    loop(batch, a_d, b_d, out, st.cuda_stream)
     e1.record(st)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     ms = e0.elapsed_time(e1)
-    res["plain_per_pair"] = {"gcups": batch.cells / (ms * 1e-3) / 1e9, "ms": ms, "wall_ms": wall * 1e3,
-                             "launches": batch.npairs}
+    return {"gcups": batch.cells / (ms * 1e-3) / 1e9, "ms": ms, "wall_ms": wall * 1e3}
+
+
+def pair_configs(roof_gcups, dev):
+    """The 4096 x 4096 uniform pair and the 131072 x 131072 mutated pair under
+    the library's default rule: best of five, GCUPS, fraction of the integer
+    roofline, and the reference's hash of the permutation."""
+    import torch
+    from . import comb_pair, pair_plan_info
+    from . import workloads as W
+    gold = _golden()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = {}
+    for name, gen, desc in (("pair_4096", W.pair_4096, "4096 x 4096, uniform {0..3}"),
+                            ("pair_131072_mutated", W.pair_131072_mutated,
+                             "131072 x 131072, b = a with 10% substitutions and 1%+1% indels")):
+        a, b = gen()
+        ad = torch.from_numpy(a).to(dev)
+        bd = torch.from_numpy(b).to(dev)
+        o = torch.empty(len(a) + len(b), dtype=torch.int32, device=dev)
+        comb_pair(ad, bd, out=o)
+        torch.cuda.synchronize()
+        runs = []
+        for _ in range(5):
+            e0.record(st)
+            comb_pair(ad, bd, out=o)
+            e1.record(st)
+            torch.cuda.synchronize()
+            runs.append(e0.elapsed_time(e1))
+        ms = min(runs)
+        g = len(a) * len(b) / (ms * 1e-3) / 1e9
+        _, c2r = strands_to_permutation(o[:len(a)], o[len(a):])
+        hv = permutation_hash(c2r.cpu().numpy())
+        want = gold.get(name, {}).get("hash")
+        res[name] = {"workload": desc, "ms": ms, "gcups": g, "roofline_frac": g / roof_gcups, "runs_ms": runs,
+                     "hash": hv, "bitexact_vs_reference": (hv == want) if want is not None else None,
+                     "variant": pair_plan_info(len(a), len(b))}
+    return res
+
+
+def costmodel_block():
+    """Regret of the installed cost model on the autotuner's held-out test
+    shapes (time of its choice over the fastest measured variant, minus one),
+    beside the fixed heuristic and the plain kernel; the model's predictions
+    run on the GPU."""
+    from . import autotune as AT
+    from . import costmodel as CM
+    model = CM.installed_model()
+    if model is None or not os.path.exists(CM.DB_PATH):
+        return None
+    import numpy as np
+    db = np.load(CM.DB_PATH)
+    rep = AT.report(model, db["test_X"], db["test_ms"])
+    return {"shapes": int(len(db["test_X"])), "variants": model.k, "variant_names": model.variants,
+            "regret": rep, "all_variants_bitexact_on_every_shape": bool(db["test_agree"].all())}
+
+
+def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev, sampler=None):
+    """Plain per-pair loops, configurations 1 and 2, the 2^20 pair (best of 5
+    runs, with the SM clocks sampled while it runs when `sampler` -- a
+    context-manager factory with a summary() -- is given), strips and braid
+    products, and the cost model's regret."""
+    import torch
+    res = {}
+    st = torch.cuda.current_stream()
+    # plain per-pair launch loops over the same batch
+    res["plain_per_pair"] = dict(_time_loop(per_pair_loop_lean, batch, a_d, b_d, out, st), launches=2 * batch.npairs,
+                                 how="slcs_comb_pair_noalloc per pair: counter reset + one wavefront launch")
+    res["plain_per_pair_alloc"] = dict(_time_loop(per_pair_loop, batch, a_d, b_d, out, st), launches=batch.npairs,
+                                       how="slcs_comb_pair per pair: plan, allocate, launch, free")
+    res["configs"] = pair_configs(roof_gcups, dev)
+    try:
+        res["costmodel"] = costmodel_block()
+    except Exception as e:  # reported, not fatal: the headline does not depend on it
+        res["costmodel"] = {"error": str(e)}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # the 2^20 x 2^20 pair: roofline fraction of the wavefront kernel
     from . import workloads as W
     a, b = W.pair_1m()
@@ -109,11 +204,7 @@ def secondary_measurements(batch, a_d, b_d, out, roof_gcups, dev, sampler=None):
     g = cells / (ms * 1e-3) / 1e9
     _, c2r = strands_to_permutation(o[:len(a)], o[len(a):])
     hv = permutation_hash(c2r.cpu().numpy())
-    gold = None
-    try:
-        gold = json.load(open(os.path.join(HERE, "..", "..", "tests", "golden", "golden.json")))["pair_1M"]["hash"]
-    except Exception:
-        pass
+    gold = _golden().get("pair_1M", {}).get("hash")
     res["long_pair"] = {"workload": "pair_1M (1048576 x 1048576, uniform {0..3})", "ms": ms, "gcups": g,
                         "roofline_frac": g / roof_gcups, "hash": hv,
                         "bitexact_vs_reference": (hv == gold) if gold is not None else None,

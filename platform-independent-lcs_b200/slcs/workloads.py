@@ -110,6 +110,10 @@ class Batch:
         b = self.b_blob[self.b_off[p]:self.b_off[p] + self.ns[p]]
         return a, b
 
+    def subset(self, indices) -> "Batch":
+        """The pairs at `indices` (in that order), packed into a batch of their own."""
+        return pack([self.pair(int(p)) for p in indices])
+
 
 def pack(pairs) -> Batch:
     """Pack a list of (a, b) uint8 arrays with 16-byte aligned offsets."""

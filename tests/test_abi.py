@@ -13,12 +13,12 @@ import slcs
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def _declared():
+def _declared(macro="SLCS_API"):
     names = set()
     for fn in os.listdir(os.path.join(ROOT, "include")):
         if fn.endswith(".h"):
             text = open(os.path.join(ROOT, "include", fn)).read()
-            names |= set(re.findall(r"SLCS_API[^;{(]*?\b(slcs_\w+)\s*\(", text))
+            names |= set(re.findall(macro + r"[^;{(]*?\b(slcs_\w+)\s*\(", text))
     return names
 
 
@@ -27,6 +27,14 @@ def test_library_exports_every_declared_symbol():
     names = _declared()
     assert len(names) >= 15
     missing = [n for n in sorted(names) if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_host_library_exports_its_c_entry_points():
+    H = slcs.host_lib()
+    names = _declared("SLCS_HOST_API")
+    assert "slcs_host_run_procedure" in names
+    missing = [n for n in sorted(names) if not hasattr(H, n)]
     assert not missing, missing
 
 
@@ -66,3 +74,23 @@ def test_argument_checks_fail_before_touching_the_device():
     assert L.slcs_batch_plan_create(ctypes.byref(ctypes.c_void_p()), big.ctypes.data, 1, None) == 6
     with pytest.raises(slcs.SlcsError):
         slcs.check(1)
+
+
+def test_noalloc_refuses_oversized_scratch_without_a_device():
+    """The allocation-free entry point refuses a pair whose scratch exceeds its
+    fixed array from the sizes alone (null pointers, no device needed)."""
+    L = slcs.lib()
+    f = L.slcs_comb_pair_noalloc
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                  ctypes.POINTER(slcs.Config), ctypes.c_void_p]
+    cfg = slcs.Config.make(tile_m=2)
+    assert f(None, 65, None, (16 << 20) // 4 + 64, None, ctypes.byref(cfg), None) == 6
+    assert b"SLCS_NOALLOC_SCRATCH_BYTES" in L.slcs_last_error()
+    assert f(None, 65, None, 1000, None, ctypes.byref(cfg), None) == 1  # fits: then the null pointers
+
+
+def test_host_adapter_unknown_procedure_without_a_device():
+    """An unknown name is the reference's impl.ok == false: reported before any
+    device work."""
+    rc, _, _, _, _, msg = slcs.run_procedure("no_such_procedure", np.zeros(3, np.int32), np.zeros(2, np.int32))
+    assert rc == 1 and "no_such_procedure" in msg
