@@ -69,7 +69,10 @@ typedef struct {
     int32_t strand_bits;   /* batch plans: 16 = combine two pairs per register where ids fit 15 bits,
                               32 = 32-bit strands only, 0 = engine default                 */
     int32_t bands;         /* row bands of a for SLCS_ALGO_STRIPS (glued by row-glue products) */
-    int32_t reserved[4];
+    int32_t pool_pct;      /* batch plans: percent of each stream class's work kept in a pool that
+                              segments claim pair by pair once their own lists are done
+                              (0 = default 15, -1 = none: every pair in a fixed list)        */
+    int32_t reserved[3];
 } slcs_config;
 
 /* One pair of a batch: symbols at a_blob[a_offset .. +m) and b_blob[b_offset .. +n);

@@ -305,6 +305,12 @@ struct StreamClass {
     bool packed;
 };
 
+// Head of a batch plan's work buffer: counters [0] wavefront ticket and [1]
+// abort, [2..3] unused, then MAX_CLASSES pool tickets (rounded up to 16);
+// the wavefront progress counters follow.
+static constexpr int WORK_HEAD = 4 + 16;
+static_assert(MAX_CLASSES <= 16, "pool tickets of every class fit the work head");
+
 struct slcs_batch_plan {
     int device = 0;
     int tm = 8;      // rows per lane of the wavefront tasks
@@ -329,6 +335,10 @@ struct slcs_batch_plan {
     int32_t *d_seg_off = nullptr;
     int32_t *d_seg_list = nullptr;
     int32_t *d_seg_list2 = nullptr;
+    int32_t *d_pool_list = nullptr;
+    int32_t *d_pool_list2 = nullptr;
+    int32_t pool_off[MAX_CLASSES + 1] = {};
+    int pool_pct = 15;
     int2 *d_tasks = nullptr;
     int64_t *d_scr_off = nullptr;
     int32_t *d_scratch = nullptr;
@@ -367,7 +377,7 @@ struct slcs_batch_plan {
         L.scratch = d_scratch;
         L.scratch_off = d_scr_off;
         L.counters = d_work;
-        L.progress = d_work + 4;
+        L.progress = d_work + WORK_HEAD;
         L.status = device_status_word();
         L.wait_ns = wait_ns;
         return L;
@@ -383,6 +393,10 @@ struct slcs_batch_plan {
                 B.class_warp_end[c] = class_warp_end[c];
                 B.class_code[c] = class_code[c];
             }
+            B.pool_list = d_pool_list;
+            B.pool_list2 = d_pool_list2;
+            B.pool_ticket = d_work + 4;
+            for (int c = 0; c <= MAX_CLASSES; ++c) B.pool_off[c] = pool_off[c];
             s = launch_batch(B, tns, st, nullptr);
         } else {
             s = launch_comb(launch(a, b, out), tm, warps, st, nullptr);
@@ -785,6 +799,7 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
                 return fail(SLCS_ERR_UNSUPPORTED, "stream mode needs tile_m in {4,8,12,16} and seg in {8,16,32}");
             }
         P->blocks_per_sm = (cfg && cfg->blocks_per_sm > 0) ? cfg->blocks_per_sm : 0;
+        if (cfg && cfg->pool_pct != 0) P->pool_pct = cfg->pool_pct < 0 ? 0 : std::min(cfg->pool_pct, 90);
     }
     for (int32_t p = 0; p < npairs; ++p) {
         if (pairs[p].m == 0 || pairs[p].n == 0) P->empty_pairs.push_back(pairs[p]);
@@ -816,7 +831,7 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
     // warp (a warp runs 32/seg segments side by side), and within a class
     // the pairs go longest first to the least loaded segment.  The grid is
     // the persistent one (or blocks_per_sm per SM), fewer for small batches.
-    std::vector<int32_t> seg_off, seg_list, seg_list2;
+    std::vector<int32_t> seg_off, seg_list, seg_list2, pool_list, pool_list2;
     if (P->stm > 0) {
         const int occ_blocks = std::max(1, full_grid / std::max(1, sm_count()));
         int grid = sm_count() * (P->blocks_per_sm > 0 ? std::min(P->blocks_per_sm, occ_blocks) : occ_blocks);
@@ -904,6 +919,7 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
         P->nclass = 0;
         long wbase = 0;
         std::vector<std::vector<std::pair<int32_t, int32_t>>> slot_lists(size_t(std::max(used, 1L)) * SEG_SLOTS);
+        std::vector<std::pair<int32_t, int32_t>> pool_items;
         for (int c = 0; c < nclass; ++c) {
             if (wc[c] == 0) continue;
             const int spw = 32 / P->classes[c].seg;
@@ -915,14 +931,28 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
                              [&](const std::pair<int32_t, int32_t> &x, const std::pair<int32_t, int32_t> &y) {
                                  return cost(c, x) > cost(c, y);
                              });
+            // Longest first to the least loaded segment until every segment
+            // holds (100 - pool_pct) % of the class's average load; the rest,
+            // the shortest items, form the class's pool, which segments claim
+            // one item at a time when their lists run out, so that the class
+            // ends evenly whatever the real speed of its segments.
+            int64_t class_cost = 0;
+            for (const auto &it : items[c]) class_cost += cost(c, it);
+            const double cap = (100 - P->pool_pct) / 100.0 * double(class_cost) / double(nseg);
+            P->pool_off[P->nclass] = int32_t(pool_items.size());
             for (const auto &it : items[c]) {
                 Load top = heap.top();
+                if (P->pool_pct > 0 && double(top.first) >= cap) {
+                    pool_items.push_back(it);
+                    continue;
+                }
                 heap.pop();
                 const long warp = wbase + top.second / spw, sidx = top.second % spw;
                 slot_lists[size_t(warp) * SEG_SLOTS + size_t(sidx)].push_back(it);
                 top.first += cost(c, it);
                 heap.push(top);
             }
+            P->pool_off[P->nclass + 1] = int32_t(pool_items.size());
             wbase += wc[c];
             if (P->classes[c].packed) P->npacked += int32_t(cls_pairs[c].size());
             P->class_warp_end[P->nclass] = int32_t(wbase);
@@ -931,6 +961,11 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
             ++P->nclass;
         }
         P->nwarps = int32_t(wbase);
+        for (int c = P->nclass + 1; c <= MAX_CLASSES; ++c) P->pool_off[c] = P->pool_off[P->nclass];
+        for (const auto &it : pool_items) {
+            pool_list.push_back(it.first);
+            pool_list2.push_back(it.second);
+        }
         if (P->nwarps > 0) {
             seg_off.reserve(size_t(P->nwarps) * SEG_SLOTS + 1);
             seg_off.push_back(0);
@@ -943,7 +978,7 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
             }
         }
     }
-    P->work_bytes = align_up(sizeof(int32_t) * (4 + S.tasks.size()), 256);
+    P->work_bytes = align_up(sizeof(int32_t) * (WORK_HEAD + S.tasks.size()), 256);
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void **ptr, size_t bytes) {
         if (e == cudaSuccess) e = cudaMalloc(ptr, bytes < 16 ? 16 : bytes);
@@ -952,6 +987,12 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
     alloc(reinterpret_cast<void **>(&P->d_seg_off), sizeof(int32_t) * seg_off.size());
     alloc(reinterpret_cast<void **>(&P->d_seg_list), sizeof(int32_t) * seg_list.size());
     alloc(reinterpret_cast<void **>(&P->d_seg_list2), sizeof(int32_t) * seg_list2.size());
+    alloc(reinterpret_cast<void **>(&P->d_pool_list), sizeof(int32_t) * pool_list.size());
+    alloc(reinterpret_cast<void **>(&P->d_pool_list2), sizeof(int32_t) * pool_list2.size());
+    if (e == cudaSuccess && !pool_list.empty())
+        e = cudaMemcpy(P->d_pool_list, pool_list.data(), sizeof(int32_t) * pool_list.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !pool_list2.empty())
+        e = cudaMemcpy(P->d_pool_list2, pool_list2.data(), sizeof(int32_t) * pool_list2.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !seg_list2.empty())
         e = cudaMemcpy(P->d_seg_list2, seg_list2.data(), sizeof(int32_t) * seg_list2.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !seg_off.empty())
@@ -1146,6 +1187,8 @@ slcs_status slcs_batch_plan_destroy(slcs_batch_plan *P)
     cudaFree(P->d_seg_off);
     cudaFree(P->d_seg_list);
     cudaFree(P->d_seg_list2);
+    cudaFree(P->d_pool_list);
+    cudaFree(P->d_pool_list2);
     cudaFree(P->d_tasks);
     cudaFree(P->d_scr_off);
     cudaFree(P->d_scratch);

@@ -421,24 +421,62 @@ __device__ __forceinline__ void take_next(const CombLaunch &L, const NextPair<TM
     }
 }
 
+// The items of one segment, in order: its list from the plan, then items of
+// its class's pool, claimed one at a time.  Only lane 0 of a segment picks;
+// lane l learns each item from lane l - 1, which switched to it one step
+// earlier (every lane of a segment sees the same column blocks, l steps
+// behind lane 0).
+struct ItemSource {
+    const int32_t *la, *lb; // the segment's list (lb: high-half pairs, packed classes only)
+    int count;              // items in the list
+    int q;                  // lane 0: position of the next item to pick
+    int cls;
+
+    __device__ __forceinline__ void pick(const BatchLaunch &B, int &pa, int &pb)
+    {
+        if (q < count) {
+            pa = la[q];
+            pb = lb ? lb[q] : -1;
+            ++q;
+            return;
+        }
+        const int off = B.pool_off[cls], size = B.pool_off[cls + 1] - off;
+        const int k = size > 0 ? atomicAdd(B.pool_ticket + cls, 1) : 0;
+        if (k < size) {
+            pa = B.pool_list[off + k];
+            pb = lb ? B.pool_list2[off + k] : -1;
+        } else {
+            pa = pb = -1;
+        }
+    }
+};
+
 template <int TM, int SEG, int TNS>
-__device__ __forceinline__ void stream_segment(const BatchLaunch &B, int seg_id, int lane)
+__device__ __forceinline__ void stream_segment(const BatchLaunch &B, int cls, int seg_id, int lane)
 {
     const CombLaunch &L = B.wf;
     const int sl = lane & (SEG - 1); // lane within the segment
     const int r0 = sl * TM;
+    const int seg_lane0 = lane & ~(SEG - 1);
     const int beg = B.seg_off[seg_id];
-    const int32_t *list = B.seg_list + beg;
-    const int count = B.seg_off[seg_id + 1] - beg;
+    ItemSource src{B.seg_list + beg, nullptr, B.seg_off[seg_id + 1] - beg, 0, cls};
 
-    int q = 0; // index of this lane's current pair in the segment's list
+    // The first two items, picked by lane 0 and shared with the segment.
+    int p0 = -1, p1 = -1, unused = -1;
+    if (sl == 0) {
+        src.pick(B, p0, unused);
+        if (p0 >= 0) src.pick(B, p1, unused);
+    }
+    p0 = __shfl_sync(FULL_MASK, p0, seg_lane0);
+    p1 = __shfl_sync(FULL_MASK, p1, seg_lane0);
     StreamTask<TM> T;
     NextPair<TM> N;
     int av[TM], hv[TM];
-    fetch_next<TM>(L, count > 0 ? list[0] : -1, r0, N);
+    fetch_next<TM>(L, p0, r0, N);
     take_next<TM>(L, N, r0, T, av, hv);
     T.nb = (T.n + TNS - 1) / TNS;
-    fetch_next<TM>(L, count > 1 ? list[1] : -1, r0, N);
+    fetch_next<TM>(L, p1, r0, N);
+    int nxt = p1; // the item after the current one (already fetched)
     int blk = -sl;
 
     int vc[TNS];
@@ -450,6 +488,7 @@ __device__ __forceinline__ void stream_segment(const BatchLaunch &B, int seg_id,
         if ((it & 3) == 0 && !__any_sync(FULL_MASK, live)) break;
         const bool act = live && blk >= 0;
         const int c = blk * TNS;
+        const int up = __shfl_up_sync(FULL_MASK, nxt, 1, SEG); // lane l - 1's next item
 
         int vi[TNS];
 #pragma unroll
@@ -499,10 +538,15 @@ __device__ __forceinline__ void stream_segment(const BatchLaunch &B, int seg_id,
 #pragma unroll
             for (int k = 0; k < TM; ++k)
                 if (r0 + k < T.m) T.h_out[T.m - 1 - r0 - k] = hv[k];
-            ++q;
             take_next<TM>(L, N, r0, T, av, hv);
             T.nb = (T.n + TNS - 1) / TNS;
-            fetch_next<TM>(L, q + 1 < count ? list[q + 1] : -1, r0, N);
+            int p = -1, unused2 = -1;
+            if (T.pair >= 0) {
+                if (sl == 0) src.pick(B, p, unused2);
+                else p = up;
+            }
+            nxt = p;
+            fetch_next<TM>(L, p, r0, N);
             blk = 0;
         }
     }
@@ -541,6 +585,8 @@ template <int TM>
 struct CoupleTask {
     int pa, pb;      // pair indices (-1: none)
     int ma, na, mb, nb_cols, nb;
+    int full_blocks; // leading blocks where both pairs have 4 columns and b is word-aligned
+    uint32_t vbase;  // (ma + 1) | (mb + 1) << 16: packed start id of column 0
     const uint8_t *ba, *bb;
     int32_t *ha, *va, *hb, *vb;
 };
@@ -577,7 +623,31 @@ __device__ __forceinline__ void take_couple(const CombLaunch &L, const NextCoupl
     T.hb = L.out + ob;
     T.vb = T.hb + T.mb;
     T.nb = (max(T.na, T.nb_cols) + 3) / 4;
+    const bool aligned = ((reinterpret_cast<uintptr_t>(T.ba) | reinterpret_cast<uintptr_t>(T.bb)) & 3) == 0;
+    T.full_blocks = (vb && aligned) ? min(T.na, T.nb_cols) / 4 : 0;
+    T.vbase = uint32_t(T.ma + 1) | (uint32_t(T.mb + 1) << 16);
     const int ra = T.ma - r0, rb = T.mb - r0;
+    if (ra >= TM && rb >= TM) {
+        // Every row of this lane lies inside both pairs: the ids of the h
+        // strands, m - r, count down by one per row in both halves at once.
+        const uint32_t hbase = uint32_t(ra) | (uint32_t(rb) << 16);
+#pragma unroll
+        for (int k = 0; k < TM; ++k) {
+            const uint32_t j = uint32_t(k % 4);
+            ap[k] = __byte_perm(N.A.sym[k / 4], N.B.sym[k / 4], j | (j << 4) | ((4 + j) << 8) | ((4 + j) << 12)) &
+                    0x00FF00FFu;
+            hp[k] = hbase - uint32_t(k) * 0x00010001u;
+        }
+        return;
+    }
+    if (ra <= 0 && rb <= 0) { // no row of this lane in either pair
+#pragma unroll
+        for (int k = 0; k < TM; ++k) {
+            ap[k] = 0x01FF01FFu;
+            hp[k] = 0u;
+        }
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < TM; ++k) {
         const uint32_t j = uint32_t(k % 4);
@@ -604,25 +674,34 @@ __device__ __forceinline__ uint32_t sym4(const uint8_t *b, int c, int n, bool &f
 }
 
 template <int TM, int SEG>
-__device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int seg_id, int lane)
+__device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int cls, int seg_id, int lane)
 {
     const CombLaunch &L = B.wf;
     const int sl = lane & (SEG - 1);
     const int r0 = sl * TM;
+    const int seg_lane0 = lane & ~(SEG - 1);
     const int beg = B.seg_off[seg_id];
-    const int32_t *la = B.seg_list + beg;
-    const int32_t *lb = B.seg_list2 + beg;
-    const int count = B.seg_off[seg_id + 1] - beg;
+    ItemSource src{B.seg_list + beg, B.seg_list2 + beg, B.seg_off[seg_id + 1] - beg, 0, cls};
 
-    int q = 0;
+    // The first two couples, picked by lane 0 and shared with the segment.
+    int a0 = -1, b0 = -1, a1 = -1, b1 = -1;
+    if (sl == 0) {
+        src.pick(B, a0, b0);
+        if (a0 >= 0) src.pick(B, a1, b1);
+    }
+    a0 = __shfl_sync(FULL_MASK, a0, seg_lane0);
+    b0 = __shfl_sync(FULL_MASK, b0, seg_lane0);
+    a1 = __shfl_sync(FULL_MASK, a1, seg_lane0);
+    b1 = __shfl_sync(FULL_MASK, b1, seg_lane0);
     CoupleTask<TM> T;
     NextCouple<TM> N;
     uint32_t ap[TM], hp[TM];
-    fetch_next<TM>(L, count > 0 ? la[0] : -1, r0, N.A);
-    fetch_next<TM>(L, count > 0 ? lb[0] : -1, r0, N.B);
+    fetch_next<TM>(L, a0, r0, N.A);
+    fetch_next<TM>(L, b0, r0, N.B);
     take_couple<TM>(L, N, r0, T, ap, hp);
-    fetch_next<TM>(L, count > 1 ? la[1] : -1, r0, N.A);
-    fetch_next<TM>(L, count > 1 ? lb[1] : -1, r0, N.B);
+    fetch_next<TM>(L, a1, r0, N.A);
+    fetch_next<TM>(L, b1, r0, N.B);
+    int nxa = a1, nxb = b1; // the couple after the current one (already fetched)
     int blk = -sl;
 
     uint32_t vc[4];
@@ -634,21 +713,38 @@ __device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int seg_i
         if ((it & 3) == 0 && !__any_sync(FULL_MASK, live)) break;
         const bool act = live && blk >= 0;
         const int c = blk * 4;
+        const int upa = __shfl_up_sync(FULL_MASK, nxa, 1, SEG); // lane l - 1's next couple
+        const int upb = __shfl_up_sync(FULL_MASK, nxb, 1, SEG);
+
+        // Blocks where both pairs have all 4 columns (and b is word-aligned)
+        // take the short forms below; the pair edges take the checked ones.
+        const bool fast = act && blk < T.full_blocks;
 
         uint32_t vi[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1, SEG);
         if (sl == 0) {
+            if (fast) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const uint32_t lo = (act && c + j < T.na) ? uint32_t(T.ma + c + j + 1) : 0x7FFFu;
-                const uint32_t hi = (act && T.pb >= 0 && c + j < T.nb_cols) ? uint32_t(T.mb + c + j + 1) : 0x7FFFu;
-                vi[j] = lo | (hi << 16);
+                for (int j = 0; j < 4; ++j) vi[j] = T.vbase + uint32_t(c + j) * 0x00010001u;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const uint32_t lo = (act && c + j < T.na) ? uint32_t(T.ma + c + j + 1) : 0x7FFFu;
+                    const uint32_t hi = (act && T.pb >= 0 && c + j < T.nb_cols) ? uint32_t(T.mb + c + j + 1) : 0x7FFFu;
+                    vi[j] = lo | (hi << 16);
+                }
             }
         }
 
         uint32_t bp[4];
-        {
+        if (fast) {
+            const uint32_t wa = __ldg(reinterpret_cast<const uint32_t *>(T.ba + c));
+            const uint32_t wb = __ldg(reinterpret_cast<const uint32_t *>(T.bb + c));
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                bp[j] = __byte_perm(wa, wb, j | (j << 4) | ((4 + j) << 8) | ((4 + j) << 12)) & 0x00FF00FFu;
+        } else {
             bool fa = false, fb = false;
             const uint32_t wa = act ? sym4(T.ba, c, T.na, fa) : 0u;
             const uint32_t wb = (act && T.pb >= 0) ? sym4(T.bb, c, T.nb_cols, fb) : 0u;
@@ -669,10 +765,18 @@ __device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int seg_i
         }
 
         if (sl == SEG - 1 && act) {
+            if (fast) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (c + j < T.na) T.va[c + j] = int32_t(vc[j] & 0xFFFFu) - 1;
-                if (T.pb >= 0 && c + j < T.nb_cols) T.vb[c + j] = int32_t(vc[j] >> 16) - 1;
+                for (int j = 0; j < 4; ++j) {
+                    T.va[c + j] = int32_t(vc[j] & 0xFFFFu) - 1;
+                    T.vb[c + j] = int32_t(vc[j] >> 16) - 1;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (c + j < T.na) T.va[c + j] = int32_t(vc[j] & 0xFFFFu) - 1;
+                    if (T.pb >= 0 && c + j < T.nb_cols) T.vb[c + j] = int32_t(vc[j] >> 16) - 1;
+                }
             }
         }
 
@@ -682,10 +786,20 @@ __device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int seg_i
                 if (r0 + k < T.ma) T.ha[T.ma - 1 - r0 - k] = int32_t(hp[k] & 0xFFFFu) - 1;
                 if (T.pb >= 0 && r0 + k < T.mb) T.hb[T.mb - 1 - r0 - k] = int32_t(hp[k] >> 16) - 1;
             }
-            ++q;
             take_couple<TM>(L, N, r0, T, ap, hp);
-            fetch_next<TM>(L, (T.pa >= 0 && q + 1 < count) ? la[q + 1] : -1, r0, N.A);
-            fetch_next<TM>(L, (T.pa >= 0 && q + 1 < count) ? lb[q + 1] : -1, r0, N.B);
+            int pa = -1, pb = -1;
+            if (T.pa >= 0) {
+                if (sl == 0) {
+                    src.pick(B, pa, pb);
+                } else {
+                    pa = upa;
+                    pb = upb;
+                }
+            }
+            nxa = pa;
+            nxb = pb;
+            fetch_next<TM>(L, pa, r0, N.A);
+            fetch_next<TM>(L, pb, r0, N.B);
             blk = 0;
         }
     }
@@ -699,8 +813,9 @@ __device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int seg_i
 // compiled into this kernel they slowed every class down by 10-15 %.)
 #define SLCS_PACKED_CLASSES(X) X(4, 16) X(8, 16) X(12, 16) X(16, 16)
 
+// Four blocks of 4 warps per SM need at most 128 registers per thread.
 template <int TNS, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) comb_batch_kernel(const BatchLaunch B)
+__global__ void __launch_bounds__(WARPS * 32, 16 / WARPS) comb_batch_kernel(const BatchLaunch B)
 {
     __shared__ __align__(16) int4 wf_ring[WARPS][RING];
     const int lane = threadIdx.x & 31;
@@ -714,14 +829,14 @@ __global__ void __launch_bounds__(WARPS * 32) comb_batch_kernel(const BatchLaunc
         const int code = B.class_code[cls];
 #define SLCS_CASE(TM, SEG)                                                                 \
     case TM * 100 + SEG:                                                                   \
-        stream_segment<TM, SEG, TNS>(B, SEG_SLOTS * gw + lane / SEG, lane);                \
+        stream_segment<TM, SEG, TNS>(B, cls, SEG_SLOTS * gw + lane / SEG, lane);                \
         break;
         switch (code) { SLCS_STREAM_CLASSES(SLCS_CASE) default: break; }
 #undef SLCS_CASE
         if (TNS == 4) {
 #define SLCS_PCASE(TM, SEG)                                                                \
     case PACKED16_CODE + TM * 100 + SEG:                                                   \
-        stream_segment16<TM, SEG>(B, SEG_SLOTS * gw + lane / SEG, lane);                   \
+        stream_segment16<TM, SEG>(B, cls, SEG_SLOTS * gw + lane / SEG, lane);                   \
         break;
             switch (code) { SLCS_PACKED_CLASSES(SLCS_PCASE) default: break; }
 #undef SLCS_PCASE

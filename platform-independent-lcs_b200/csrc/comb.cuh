@@ -54,6 +54,12 @@ struct BatchLaunch {
     int32_t nclass;          // stream classes; warp w serves the first class c with w < class_warp_end[c]
     int32_t class_warp_end[MAX_CLASSES];
     int32_t class_code[MAX_CLASSES]; // rows per lane * 100 + lanes per segment (+ PACKED16_CODE when packed)
+    // Pool of each class: items no segment list holds, claimed one at a time
+    // (pool_ticket[c]) by segments of class c whose own lists are done.
+    const int32_t *pool_list;        // device: pairs (packed classes: the low-half pair)
+    const int32_t *pool_list2;       // device: packed classes: the high-half pair (-1: none)
+    int32_t *pool_ticket;            // device: MAX_CLASSES counters, zero at launch
+    int32_t pool_off[MAX_CLASSES + 1]; // CSR offsets of the classes' pools
 };
 // Class-code offset of the packed variant: two pairs per register, strand ids
 // in 15 bits (pairs with m + n <= PACKED16_MAX_IDS), 4 columns per step.

@@ -32,7 +32,7 @@ class Config(ctypes.Structure):
                 ("warps", ctypes.c_int32), ("braid_cutoff", ctypes.c_int32), ("strips", ctypes.c_int32),
                 ("use_graph", ctypes.c_int32), ("seg", ctypes.c_int32), ("wait_ms", ctypes.c_int32),
                 ("blocks_per_sm", ctypes.c_int32), ("strand_bits", ctypes.c_int32), ("bands", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 4)]
+                ("pool_pct", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
 
     @classmethod
     def make(cls, **kw) -> "Config":
