@@ -65,13 +65,15 @@ typedef struct {
     int32_t use_graph;     /* batch plans: replay the launch as a captured CUDA graph */
     int32_t seg;           /* batch stream mode: lanes per pipeline segment (8/16/32) */
     int32_t wait_ms;       /* limit of one device-side wait (default 10000 ms)        */
-    int32_t blocks_per_sm; /* batch plans: resident blocks per SM (default: occupancy) */
+    int32_t blocks_per_sm; /* batch plans: resident blocks per SM (default: 2 for plans with packed
+                              pairs, else as many as fit)                                 */
     int32_t strand_bits;   /* batch plans: 16 = combine two pairs per register where ids fit 15 bits,
                               32 = 32-bit strands only, 0 = engine default                 */
     int32_t bands;         /* row bands of a for SLCS_ALGO_STRIPS (glued by row-glue products) */
     int32_t pool_pct;      /* batch plans: percent of each stream class's work kept in a pool that
                               segments claim pair by pair once their own lists are done
-                              (0 = default 15, -1 = none: every pair in a fixed list)        */
+                              (0 = default: 50 for plans with packed pairs, else 15;
+                              -1 = none: every pair in a fixed list)        */
     int32_t reserved[3];
 } slcs_config;
 

@@ -305,6 +305,30 @@ struct StreamClass {
     bool packed;
 };
 
+// Relative time of one step of a warp of a stream class (all its segments
+// advance one column block), which sets how many warps the class gets.  A
+// warp's pace is not its own instruction count: the warps of an SM
+// sub-partition share its issue slots and integer pipe, so the classes differ
+// less than their rows per lane do.  Fitted to B200 per-warp clocks of the
+// 20,000 read/window pairs (4 columns per step, 8 warps per SM): packed
+// classes of 4, 8, 12 and 16 rows per lane 1554, 1327, 1392 and 1909 ns per
+// step, 32-bit 32-lane classes of 12 and 16 rows 1348 and 1500 ns.  Plans
+// with 8 columns per step weigh every class alike (no measurements).
+static double class_step_time(const StreamClass &k, int tns)
+{
+    if (tns != 4) return 1.0;
+    if (k.packed) {
+        switch (k.tm) {
+        case 4: return 1554.0;
+        case 8: return 1327.0;
+        case 12: return 1392.0;
+        default: return 1909.0;
+        }
+    }
+    if (k.seg == 32) return k.tm <= 12 ? 1348.0 : 1500.0;
+    return 1000.0 + 30.0 * k.tm; // 16-lane 32-bit classes: between the two above
+}
+
 // Head of a batch plan's work buffer: counters [0] wavefront ticket and [1]
 // abort, [2..3] unused, then MAX_CLASSES pool tickets (rounded up to 16);
 // the wavefront progress counters follow.
@@ -798,7 +822,17 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
                 delete P;
                 return fail(SLCS_ERR_UNSUPPORTED, "stream mode needs tile_m in {4,8,12,16} and seg in {8,16,32}");
             }
-        P->blocks_per_sm = (cfg && cfg->blocks_per_sm > 0) ? cfg->blocks_per_sm : 0;
+        // Packed plans: 8 warps per SM and half of each class's work in its
+        // pool.  A packed item is a couple of pairs, and with 16 warps per SM
+        // a segment combed only one or two of them, so the launch ended with
+        // whichever segments drew two; at 8 warps per SM each warp runs
+        // twice as fast and combs twice as many items (20,000 reads on B200:
+        // 0.381 -> 0.328 ms).  32-bit plans keep the full occupancy (2 blocks
+        // per SM: 0.361 -> 0.420 ms) and a 15 % pool.
+        const bool packed_plan = pack && std::any_of(P->classes.begin(), P->classes.end(),
+                                                     [](const StreamClass &k) { return k.packed; });
+        P->blocks_per_sm = (cfg && cfg->blocks_per_sm > 0) ? cfg->blocks_per_sm : (packed_plan ? 2 : 0);
+        P->pool_pct = packed_plan ? 50 : 15;
         if (cfg && cfg->pool_pct != 0) P->pool_pct = cfg->pool_pct < 0 ? 0 : std::min(cfg->pool_pct, 90);
     }
     for (int32_t p = 0; p < npairs; ++p) {
@@ -864,9 +898,6 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
             }
         }
         // Cost of an item: its column blocks plus a pair switch, in steps.
-        // (Weighting steps by the instructions of a class made the plans
-        // slower on the GPU: a warp's speed is not set by its own share of
-        // the integer pipes alone.)
         auto cost = [&](int c, const std::pair<int32_t, int32_t> &it) {
             const int cols = P->classes[c].packed ? 4 : P->tns;
             const int32_t n = std::max(pairs[it.first].n, it.second >= 0 ? pairs[it.second].n : 0);
@@ -879,7 +910,7 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
             int64_t w = 0;
             for (const auto &it : items[c]) w += cost(c, it);
             const int spw = 32 / P->classes[c].seg;
-            wsteps[c] = double(w) / spw;
+            wsteps[c] = double(w) / spw * class_step_time(P->classes[c], P->tns);
             wmax[c] = (long(items[c].size()) + spw - 1) / spw;
             total += wsteps[c];
         }

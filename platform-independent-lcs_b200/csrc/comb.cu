@@ -425,27 +425,36 @@ __device__ __forceinline__ void take_next(const CombLaunch &L, const NextPair<TM
 // its class's pool, claimed one at a time.  Only lane 0 of a segment picks;
 // lane l learns each item from lane l - 1, which switched to it one step
 // earlier (every lane of a segment sees the same column blocks, l steps
-// behind lane 0).
+// behind lane 0).  Lane 0 claims its pool tickets one pick ahead, so that the
+// atomic's round trip overlaps a whole pair instead of stalling the warp.
 struct ItemSource {
     const int32_t *la, *lb; // the segment's list (lb: high-half pairs, packed classes only)
     int count;              // items in the list
     int q;                  // lane 0: position of the next item to pick
     int cls;
+    int ahead;              // lane 0: pool ticket claimed for the next pick (-1: none yet)
+
+    __device__ __forceinline__ int claim(const BatchLaunch &B, int size) const
+    {
+        return size > 0 ? atomicAdd(B.pool_ticket + cls, 1) : 0;
+    }
 
     __device__ __forceinline__ void pick(const BatchLaunch &B, int &pa, int &pb)
     {
+        const int off = B.pool_off[cls], size = B.pool_off[cls + 1] - off;
         if (q < count) {
             pa = la[q];
             pb = lb ? lb[q] : -1;
-            ++q;
+            if (++q == count && ahead < 0) ahead = claim(B, size);
             return;
         }
-        const int off = B.pool_off[cls], size = B.pool_off[cls + 1] - off;
-        const int k = size > 0 ? atomicAdd(B.pool_ticket + cls, 1) : 0;
+        const int k = ahead >= 0 ? ahead : claim(B, size);
         if (k < size) {
+            ahead = claim(B, size);
             pa = B.pool_list[off + k];
             pb = lb ? B.pool_list2[off + k] : -1;
         } else {
+            ahead = size;
             pa = pb = -1;
         }
     }
@@ -459,7 +468,7 @@ __device__ __forceinline__ void stream_segment(const BatchLaunch &B, int cls, in
     const int r0 = sl * TM;
     const int seg_lane0 = lane & ~(SEG - 1);
     const int beg = B.seg_off[seg_id];
-    ItemSource src{B.seg_list + beg, nullptr, B.seg_off[seg_id + 1] - beg, 0, cls};
+    ItemSource src{B.seg_list + beg, nullptr, B.seg_off[seg_id + 1] - beg, 0, cls, -1};
 
     // The first two items, picked by lane 0 and shared with the segment.
     int p0 = -1, p1 = -1, unused = -1;
@@ -681,7 +690,7 @@ __device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int cls, 
     const int r0 = sl * TM;
     const int seg_lane0 = lane & ~(SEG - 1);
     const int beg = B.seg_off[seg_id];
-    ItemSource src{B.seg_list + beg, B.seg_list2 + beg, B.seg_off[seg_id + 1] - beg, 0, cls};
+    ItemSource src{B.seg_list + beg, B.seg_list2 + beg, B.seg_off[seg_id + 1] - beg, 0, cls, -1};
 
     // The first two couples, picked by lane 0 and shared with the segment.
     int a0 = -1, b0 = -1, a1 = -1, b1 = -1;
