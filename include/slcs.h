@@ -251,6 +251,20 @@ SLCS_API slcs_status slcs_permutation_to_strands(const int32_t *row_to_col, int3
 SLCS_API slcs_status slcs_substring_llcs(const int32_t *v_strands, int32_t m, int32_t n, const int32_t *begin,
                                          const int32_t *end, int32_t nq, int32_t *llcs_out, void *stream);
 
+/* PermutationMatrix::hash (src/permutation_matrix.hpp:192-203) of
+ * FromStrands(h, v) (88-115), on the device, with no permutation array
+ * written: the chain over v then h, with the reference's signed 64-bit
+ * wrap.  *hash_out is a device int64.  The chain is sequential (one GPU
+ * thread; a long pair hashes faster on the host, slcs_permutation_hash). */
+SLCS_API slcs_status slcs_strands_hash(const int32_t *h, int32_t m, const int32_t *v, int32_t n, int64_t *hash_out,
+                                       void *stream);
+/* The hash of every pair of a batch from the plan's output blob (device
+ * pointers; hashes_out has one int64 per pair, in descriptor order), one
+ * chain per GPU thread: what the reference's driver records per run
+ * (src/main.cpp:58-64), for all pairs at once. */
+SLCS_API slcs_status slcs_batch_plan_hash(const slcs_batch_plan *plan, const int32_t *strands, int64_t *hashes_out,
+                                          void *stream);
+
 /* PermutationMatrix::hash (src/permutation_matrix.hpp:192-203) of a host
  * col_to_row array, with the reference's signed 64-bit wrap-around. */
 SLCS_API int64_t slcs_permutation_hash(const int32_t *col_to_row, int32_t size);

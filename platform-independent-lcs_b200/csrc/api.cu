@@ -1313,6 +1313,23 @@ slcs_status slcs_permutation_to_strands(const int32_t *row_to_col, int32_t m, in
     return perm_to_strands(row_to_col, m, n, h, v, static_cast<cudaStream_t>(stream));
 }
 
+slcs_status slcs_strands_hash(const int32_t *h, int32_t m, const int32_t *v, int32_t n, int64_t *hash_out,
+                              void *stream)
+{
+    if (m < 0 || n < 0) return fail(SLCS_ERR_INVALID, "m and n must be >= 0");
+    if (int64_t(m) + n > INT32_MAX) return fail(SLCS_ERR_RANGE, "m+n exceeds int32 strand ids");
+    if ((m > 0 && !h) || (n > 0 && !v) || !hash_out) return fail(SLCS_ERR_INVALID, "null strands or output");
+    return launch_strands_hash(h, m, v, n, hash_out, static_cast<cudaStream_t>(stream));
+}
+
+slcs_status slcs_batch_plan_hash(const slcs_batch_plan *P, const int32_t *strands, int64_t *hashes_out,
+                                 void *stream)
+{
+    if (!P) return fail(SLCS_ERR_INVALID, "plan is null");
+    if (P->npairs > 0 && (!strands || !hashes_out)) return fail(SLCS_ERR_INVALID, "null strands or output");
+    return launch_batch_hash(P->d_pairs, P->npairs, strands, hashes_out, static_cast<cudaStream_t>(stream));
+}
+
 // Restates PermutationMatrix::hash (src/permutation_matrix.hpp:192-203): the
 // reference multiplies in signed 64-bit and its build wraps on overflow, so
 // the wrap is reproduced in unsigned arithmetic; % truncates toward zero.

@@ -104,6 +104,14 @@ slcs_status launch_batch(const BatchLaunch &L, int tns, cudaStream_t stream, int
 constexpr int BATCH_WARPS = 4;
 constexpr int BATCH_WF_TM = 8;
 
+// PermutationMatrix::hash of FromStrands(h, v) (hash.cu): one chain per
+// thread; *out (device) receives it.
+slcs_status launch_strands_hash(const int32_t *h, int32_t m, const int32_t *v, int32_t n, int64_t *out,
+                                cudaStream_t st);
+// The same for every pair of a batch (device descriptors): out[p].
+slcs_status launch_batch_hash(const PairDev *pairs, int32_t npairs, const int32_t *strands, int64_t *out,
+                              cudaStream_t st);
+
 // Strands -> permutation matrix arrays (either output may be null).
 slcs_status launch_strands_to_perm(const int32_t *h, int32_t m, const int32_t *v, int32_t n,
                                    int32_t *row_to_col, int32_t *col_to_row, cudaStream_t stream);

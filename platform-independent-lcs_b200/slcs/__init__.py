@@ -110,6 +110,8 @@ def lib():
         L.slcs_probe_int_rates.argtypes = [_i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _vp]
         L.slcs_braid_multiply.argtypes = [_vp, _i32, _vp, _i32, _i32, _i32, _vp, ctypes.POINTER(Config), _vp]
         L.slcs_probe_wait_expiry.argtypes = [_i32, _vp]
+        L.slcs_strands_hash.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp]
+        L.slcs_batch_plan_hash.argtypes = [_vp, _vp, _vp, _vp]
         L.slcs_symbols_to_bytes.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, _vp, _vp]
         L.slcs_comb_pair_words_host.argtypes = [_vp, _i32, _vp, _i32, _vp, _vp, ctypes.POINTER(Config)]
         L.slcs_comb_pair_noalloc.argtypes = [_vp, _i32, _vp, _i32, _vp, ctypes.POINTER(Config), _vp]
@@ -283,6 +285,15 @@ class BatchPlan:
         check(lib().slcs_batch_plan_run_host(self._h, a_blob.ctypes.data, a_blob.size, b_blob.ctypes.data,
                                              b_blob.size, out.ctypes.data, out.size, _stream(stream)))
 
+    def hashes(self, out, stream=None):
+        """PermutationMatrix::hash of every pair's strands in the plan's output
+        blob `out` (int32 CUDA tensor), computed on the device: an int64
+        CUDA tensor with one hash per pair."""
+        import torch
+        h = torch.empty(len(self._descs), dtype=torch.int64, device=out.device)
+        check(lib().slcs_batch_plan_hash(self._h, _dptr(out), _dptr(h), _stream(stream)))
+        return h
+
     def close(self):
         if self._h:
             lib().slcs_batch_plan_destroy(self._h)
@@ -346,6 +357,15 @@ def substring_llcs(v, m: int, begin, end, stream=None):
     check(lib().slcs_substring_llcs(_dptr(v), int(m), int(v.numel()), _dptr(begin), _dptr(end), nq, _dptr(out),
                                     _stream(stream)))
     return out
+
+
+def strands_hash(h, v, stream=None) -> int:
+    """PermutationMatrix::hash of FromStrands(h, v) computed on the device."""
+    import torch
+    out = torch.empty(1, dtype=torch.int64, device=h.device)
+    check(lib().slcs_strands_hash(_dptr(h), int(h.numel()), _dptr(v), int(v.numel()), out.data_ptr(),
+                                  _stream(stream)))
+    return int(out.item())
 
 
 def permutation_hash(col_to_row: np.ndarray) -> int:
