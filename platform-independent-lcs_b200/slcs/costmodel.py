@@ -24,28 +24,52 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 MODEL_PATH = os.path.join(HERE, "data", "costmodel.json")
 DB_PATH = os.path.join(HERE, "data", "timings.npz")
 
-# The variants the autotuner times and the model ranks.  Variant 0 is what the
-# library does when nothing is configured (the fixed heuristic).
+# The variants the autotuner times and the model ranks.  "batch" variants are
+# launch plans of one batch (slcs_batch_plan_*); "pair" variants comb each
+# pair of a shape with slcs_comb_pair under a tiling and a steady-ant cutoff
+# (src/braid_multiplication.hpp:204-270 is the recursion whose base case the
+# cutoff moves), and apply to shapes of at most PAIR_BATCH_MAX pairs.
+# Variant 0 is what the library does for a batch when nothing is configured.
+PAIR_BATCH_MAX = 8
 VARIANTS: List[dict] = [
-    {"name": "stream_auto", "cfg": {}},
-    {"name": "stream_tn8_32", "cfg": {"strand_bits": 32}},
-    {"name": "stream_tn4_32", "cfg": {"strand_bits": 32, "tile_n": 4}},
-    {"name": "stream_auto_bpsm2", "cfg": {"blocks_per_sm": 2}},
-    {"name": "stream_tn8_32_bpsm2", "cfg": {"strand_bits": 32, "blocks_per_sm": 2}},
-    {"name": "wavefront_tm2", "cfg": {"algo": 1, "tile_m": 2}},
-    {"name": "wavefront_tm4", "cfg": {"algo": 1, "tile_m": 4}},
-    {"name": "wavefront_tm8", "cfg": {"algo": 1, "tile_m": 8}},
-    {"name": "wavefront_tm16", "cfg": {"algo": 1, "tile_m": 16}},
-    {"name": "wavefront_tm16_w8", "cfg": {"algo": 1, "tile_m": 16, "warps": 8}},
-    {"name": "wavefront_tm8_w8", "cfg": {"algo": 1, "tile_m": 8, "warps": 8}},
+    {"name": "stream_auto", "kind": "batch", "cfg": {}},
+    {"name": "stream_tn8_32", "kind": "batch", "cfg": {"strand_bits": 32}},
+    {"name": "stream_tn4_32", "kind": "batch", "cfg": {"strand_bits": 32, "tile_n": 4}},
+    {"name": "stream_auto_bpsm4", "kind": "batch", "cfg": {"blocks_per_sm": 4}},
+    {"name": "stream_tn8_32_bpsm2", "kind": "batch", "cfg": {"strand_bits": 32, "blocks_per_sm": 2}},
+    {"name": "wavefront_tm2", "kind": "batch", "cfg": {"algo": 1, "tile_m": 2}},
+    {"name": "wavefront_tm4", "kind": "batch", "cfg": {"algo": 1, "tile_m": 4}},
+    {"name": "wavefront_tm8", "kind": "batch", "cfg": {"algo": 1, "tile_m": 8}},
+    {"name": "wavefront_tm16", "kind": "batch", "cfg": {"algo": 1, "tile_m": 16}},
+    {"name": "wavefront_tm16_w8", "kind": "batch", "cfg": {"algo": 1, "tile_m": 16, "warps": 8}},
+    {"name": "wavefront_tm8_w8", "kind": "batch", "cfg": {"algo": 1, "tile_m": 8, "warps": 8}},
+] + [
+    {"name": f"pair_auto_c{c}", "kind": "pair", "cfg": {"braid_cutoff": c}} for c in (64, 256, 1024, 4096)
+] + [
+    {"name": f"pair_strips{s}_c{c}", "kind": "pair", "cfg": {"algo": 2, "strips": s, "bands": 1, "braid_cutoff": c}}
+    for s in (2, 4, 8, 16) for c in (256, 1024)
+] + [
+    {"name": f"pair_bands{r}_c{c}", "kind": "pair", "cfg": {"algo": 2, "strips": 1, "bands": r, "braid_cutoff": c}}
+    for r in (2, 4, 8) for c in (256, 1024)
 ]
 HEURISTIC = 0
 PLAIN = 7  # the plain wavefront kernel with its default tile
+PAIR_DEFAULT = [v["name"] for v in VARIANTS].index("pair_auto_c256")  # the library's rule for one pair
+
+
+def is_pair(i: int) -> bool:
+    return VARIANTS[i]["kind"] == "pair"
+
+
+def applicable(batch: float) -> np.ndarray:
+    """Which variants apply to a shape of `batch` pairs (pair variants comb
+    the pairs one call each, so they are offered for small batches only)."""
+    return np.array([not is_pair(i) or batch <= PAIR_BATCH_MAX for i in range(len(VARIANTS))])
 
 
 def variant_config(i: int, use_graph: bool = True) -> Config:
     kw = dict(VARIANTS[i]["cfg"])
-    if use_graph:
+    if use_graph and not is_pair(i):
         kw["use_graph"] = 1
     return Config.make(**kw)
 
@@ -144,7 +168,12 @@ class CostModel:
         return predict(self.params, self.k, X)
 
     def choose_index(self, X) -> np.ndarray:
-        return np.argmin(self.predict(X), axis=1)
+        """Fastest predicted applicable variant per row of X (features; the
+        batch size is 2 ** X[:, 3])."""
+        X = np.asarray(X, np.float32).reshape(-1, 4)
+        Y = self.predict(X)
+        ok = np.stack([applicable(2.0 ** float(x[3])) for x in X])
+        return np.argmin(np.where(ok, Y, np.inf), axis=1)
 
     def save(self, path: str = MODEL_PATH, extra: Optional[dict] = None):
         os.makedirs(os.path.dirname(path), exist_ok=True)
@@ -176,15 +205,19 @@ def installed_model() -> Optional[CostModel]:
     return _MODEL or None
 
 
-def ranking(batch) -> Optional[np.ndarray]:
-    """Variant indices, fastest predicted first (None without a model)."""
+def ranking(batch, kind: Optional[str] = None) -> Optional[np.ndarray]:
+    """Applicable variant indices (of `kind` "batch" or "pair" when given),
+    fastest predicted first (None without a model)."""
     model = installed_model()
     if model is None:
         return None
-    return np.argsort(model.predict(batch_features(batch)[None, :])[0], kind="stable")
+    x = batch_features(batch)
+    order = np.argsort(model.predict(x[None, :])[0], kind="stable")
+    ok = applicable(batch.npairs)
+    return np.array([int(i) for i in order if ok[i] and (kind is None or VARIANTS[int(i)]["kind"] == kind)])
 
 
 def choose(batch) -> Optional[Config]:
-    """The model's variant for a batch, or None when no model is installed."""
-    r = ranking(batch)
+    """The model's batch-plan variant for a batch, or None when no model is installed."""
+    r = ranking(batch, kind="batch")
     return None if r is None else variant_config(int(r[0]))

@@ -10,6 +10,8 @@ import json
 import os
 import time
 
+import numpy as np
+
 from . import Config, check, lib, strands_to_permutation, permutation_hash
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -31,7 +33,7 @@ def choose_batch_config(batch, timer=None, top: int = 3):
     heuristic."""
     try:
         from . import costmodel
-        order = costmodel.ranking(batch)
+        order = costmodel.ranking(batch, kind="batch")
     except Exception:
         order = None
     if order is None:
@@ -42,6 +44,27 @@ def choose_batch_config(batch, timer=None, top: int = 3):
     times = {}
     for i in order[:top]:
         times[costmodel.VARIANTS[int(i)]["name"]] = float(timer(costmodel.variant_config(int(i))))
+    best = min(times, key=times.get)
+    idx = [v["name"] for v in costmodel.VARIANTS].index(best)
+    return (costmodel.variant_config(idx), f"cost_model_top{top}_timed",
+            {"model_choice": names[0], "candidates_ms": times, "chosen": best})
+
+
+def choose_pair_config(m: int, n: int, sigma: int, timer=None, top: int = 3):
+    """(config, how it was chosen, details) for one m x n pair: the cost
+    model's best-ranked single-pair variant (tiling and steady-ant cutoff), or
+    with `timer` the fastest of its `top` best-ranked ones, measured; without
+    a model, the library's own rule (Config())."""
+    from . import costmodel
+    model = costmodel.installed_model()
+    if model is None:
+        return Config.make(), "library_rule", {}
+    y = model.predict(costmodel.features_of(m, n, sigma, 1)[None, :])[0]
+    order = [int(i) for i in np.argsort(y, kind="stable") if costmodel.is_pair(int(i))]
+    names = [costmodel.VARIANTS[i]["name"] for i in order[:top]]
+    if timer is None:
+        return costmodel.variant_config(order[0]), "cost_model", {"model_choice": names[0]}
+    times = {costmodel.VARIANTS[i]["name"]: float(timer(costmodel.variant_config(i))) for i in order[:top]}
     best = min(times, key=times.get)
     idx = [v["name"] for v in costmodel.VARIANTS].index(best)
     return (costmodel.variant_config(idx), f"cost_model_top{top}_timed",
@@ -138,6 +161,30 @@ def pair_configs(roof_gcups, dev):
         res[name] = {"workload": desc, "ms": ms, "gcups": g, "roofline_frac": g / roof_gcups, "runs_ms": runs,
                      "hash": hv, "bitexact_vs_reference": (hv == want) if want is not None else None,
                      "variant": pair_plan_info(len(a), len(b))}
+
+        # the cost model's single-pair variant (its three best-ranked, timed)
+        def timer(cfg):
+            comb_pair(ad, bd, cfg=cfg, out=o)
+            torch.cuda.synchronize()
+            best = float("inf")
+            for _ in range(3):
+                e0.record(st)
+                comb_pair(ad, bd, cfg=cfg, out=o)
+                e1.record(st)
+                torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            return best
+
+        cfg, how, info = choose_pair_config(len(a), len(b), 4, timer=timer)
+        if how != "library_rule":
+            tms = min(info["candidates_ms"].values())
+            comb_pair(ad, bd, cfg=cfg, out=o)
+            _, c2r = strands_to_permutation(o[:len(a)], o[len(a):])
+            thv = permutation_hash(c2r.cpu().numpy())
+            tg = len(a) * len(b) / (tms * 1e-3) / 1e9
+            res[name]["tuned"] = {"ms": tms, "gcups": tg, "roofline_frac": tg / roof_gcups, "how": how,
+                                  "tuning": info, "bitexact_vs_reference": (thv == want) if want is not None else None,
+                                  "variant": pair_plan_info(len(a), len(b), cfg)}
     return res
 
 
