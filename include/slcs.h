@@ -207,6 +207,14 @@ SLCS_API slcs_status slcs_batch_plan_run(slcs_batch_plan *plan, const uint8_t *a
 SLCS_API slcs_status slcs_batch_plan_run_host(slcs_batch_plan *plan, const uint8_t *a_blob, int64_t a_len,
                                               const uint8_t *b_blob, int64_t b_len, int32_t *out, int64_t out_len,
                                               void *stream);
+/* The same with the strands returned as int16 (ids of pairs with
+ * m + n <= 32767 fit; a plan with a larger pair gives SLCS_ERR_RANGE): the
+ * strands are narrowed on the device, so half the bytes cross the bus.  The
+ * values are those of slcs_batch_plan_run_host.  No counterpart in the
+ * reference, whose strands are int32 Words. */
+SLCS_API slcs_status slcs_batch_plan_run_host16(slcs_batch_plan *plan, const uint8_t *a_blob, int64_t a_len,
+                                                const uint8_t *b_blob, int64_t b_len, int16_t *out, int64_t out_len,
+                                                void *stream);
 SLCS_API slcs_status slcs_batch_plan_destroy(slcs_batch_plan *plan);
 /* Kernel launches one slcs_batch_plan_run issues (for launch accounting). */
 SLCS_API int32_t slcs_batch_plan_launches(const slcs_batch_plan *plan);

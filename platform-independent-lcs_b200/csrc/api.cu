@@ -374,6 +374,10 @@ struct slcs_batch_plan {
     cudaStream_t cap_stream = nullptr;
     // Extents the descriptors reach (elements), checked by the host-pointer run.
     int64_t need_a = 0, need_b = 0, need_out = 0;
+    int64_t max_ids = 0; // largest m + n of a pair (strand ids are below it)
+    // Device int16 copy of the strands for slcs_batch_plan_run_host16, grown on demand.
+    int16_t *d_out16 = nullptr;
+    size_t out16_elems = 0;
     // Device staging of slcs_batch_plan_run_host, grown on demand.
     char *h_stage = nullptr;
     size_t h_stage_bytes = 0;
@@ -840,6 +844,7 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
         P->need_a = std::max<int64_t>(P->need_a, pairs[p].a_offset + pairs[p].m);
         P->need_b = std::max<int64_t>(P->need_b, pairs[p].b_offset + pairs[p].n);
         P->need_out = std::max<int64_t>(P->need_out, pairs[p].out_offset + pairs[p].m + pairs[p].n);
+        P->max_ids = std::max<int64_t>(P->max_ids, int64_t(pairs[p].m) + pairs[p].n);
     }
     int32_t stream_rows = 0;
     for (const auto &c : P->classes) stream_rows = std::max(stream_rows, c.tm * c.seg);
@@ -1203,9 +1208,95 @@ slcs_status slcs_batch_plan_run_host(slcs_batch_plan *P, const uint8_t *a, int64
     return slcs_device_status(P->device, 1);
 }
 
+// The strands of [lo, hi) narrowed to int16 (every id of the plan is below 2^15).
+__global__ void narrow16_kernel(const int32_t *__restrict__ in, int16_t *__restrict__ out, int64_t lo, int64_t hi)
+{
+    for (int64_t i = lo + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < hi; i += int64_t(gridDim.x) * blockDim.x)
+        out[i] = int16_t(in[i]);
+}
+
+static slcs_status narrow16(const int32_t *in, int16_t *out, int64_t lo, int64_t hi, cudaStream_t st)
+{
+    if (hi <= lo) return SLCS_OK;
+    const int blocks = int(std::min<int64_t>((hi - lo + 255) / 256, int64_t(sm_count()) * 8));
+    narrow16_kernel<<<blocks, 256, 0, st>>>(in, out, lo, hi);
+    SLCS_CUDA(cudaGetLastError());
+    return SLCS_OK;
+}
+
+slcs_status slcs_batch_plan_run_host16(slcs_batch_plan *P, const uint8_t *a, int64_t a_len, const uint8_t *b,
+                                       int64_t b_len, int16_t *out, int64_t out_len, void *stream)
+{
+    if (!P) return fail(SLCS_ERR_INVALID, "plan is null");
+    if (P->max_ids > 32767) return fail(SLCS_ERR_RANGE, "a pair of the plan has m + n > 32767: ids need int32");
+    if (a_len < P->need_a || b_len < P->need_b || out_len < P->need_out)
+        return fail(SLCS_ERR_RANGE, "a host buffer is shorter than the plan's descriptors reach");
+    if ((P->need_a && !a) || (P->need_b && !b) || (P->need_out && !out))
+        return fail(SLCS_ERR_INVALID, "null host buffer");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t ab = align_up(size_t(P->need_a) + 16, 256), bb = align_up(size_t(P->need_b) + 16, 256);
+    const size_t need = ab + bb + sizeof(int32_t) * size_t(P->need_out) + 16;
+    if (need > P->h_stage_bytes || size_t(P->need_out) > P->out16_elems) {
+        SLCS_CUDA(cudaStreamSynchronize(st));
+        if (need > P->h_stage_bytes) {
+            cudaFree(P->h_stage);
+            P->h_stage = nullptr;
+            P->h_stage_bytes = 0;
+            SLCS_CUDA(cudaMalloc(reinterpret_cast<void **>(&P->h_stage), need));
+            P->h_stage_bytes = need;
+        }
+        if (size_t(P->need_out) > P->out16_elems) {
+            cudaFree(P->d_out16);
+            P->d_out16 = nullptr;
+            P->out16_elems = 0;
+            SLCS_CUDA(cudaMalloc(reinterpret_cast<void **>(&P->d_out16), sizeof(int16_t) * size_t(P->need_out) + 16));
+            P->out16_elems = size_t(P->need_out);
+        }
+    }
+    uint8_t *da = reinterpret_cast<uint8_t *>(P->h_stage);
+    uint8_t *db = reinterpret_cast<uint8_t *>(P->h_stage + ab);
+    int32_t *dout = reinterpret_cast<int32_t *>(P->h_stage + ab + bb);
+    int16_t *d16 = P->d_out16;
+    if (!P->chunks.empty()) {
+        // As slcs_batch_plan_run_host, chunk by chunk on their own streams,
+        // with each chunk's strands narrowed on the device before they cross
+        // the bus (half the bytes of the copy back).
+        SLCS_CUDA(cudaEventRecord(P->chunk_start, st));
+        for (auto &k : P->chunks) {
+            SLCS_CUDA(cudaStreamWaitEvent(k.stream, P->chunk_start, 0));
+            if (k.a_hi > k.a_lo)
+                SLCS_CUDA(cudaMemcpyAsync(da + k.a_lo, a + k.a_lo, size_t(k.a_hi - k.a_lo), cudaMemcpyHostToDevice,
+                                          k.stream));
+            if (k.b_hi > k.b_lo)
+                SLCS_CUDA(cudaMemcpyAsync(db + k.b_lo, b + k.b_lo, size_t(k.b_hi - k.b_lo), cudaMemcpyHostToDevice,
+                                          k.stream));
+            slcs_status s = slcs_batch_plan_run(k.plan, da, db, dout, k.stream);
+            if (s == SLCS_OK) s = narrow16(dout, d16, k.o_lo, k.o_hi, k.stream);
+            if (s != SLCS_OK) return s;
+            if (k.o_hi > k.o_lo)
+                SLCS_CUDA(cudaMemcpyAsync(out + k.o_lo, d16 + k.o_lo, sizeof(int16_t) * size_t(k.o_hi - k.o_lo),
+                                          cudaMemcpyDeviceToHost, k.stream));
+            SLCS_CUDA(cudaEventRecord(k.done, k.stream));
+            SLCS_CUDA(cudaStreamWaitEvent(st, k.done, 0));
+        }
+        SLCS_CUDA(cudaStreamSynchronize(st));
+        return slcs_device_status(P->device, 1);
+    }
+    if (P->need_a) SLCS_CUDA(cudaMemcpyAsync(da, a, size_t(P->need_a), cudaMemcpyHostToDevice, st));
+    if (P->need_b) SLCS_CUDA(cudaMemcpyAsync(db, b, size_t(P->need_b), cudaMemcpyHostToDevice, st));
+    slcs_status s = slcs_batch_plan_run(P, da, db, dout, stream);
+    if (s == SLCS_OK) s = narrow16(dout, d16, 0, P->need_out, st);
+    if (s != SLCS_OK) return s;
+    if (P->need_out)
+        SLCS_CUDA(cudaMemcpyAsync(out, d16, sizeof(int16_t) * size_t(P->need_out), cudaMemcpyDeviceToHost, st));
+    SLCS_CUDA(cudaStreamSynchronize(st));
+    return slcs_device_status(P->device, 1);
+}
+
 slcs_status slcs_batch_plan_destroy(slcs_batch_plan *P)
 {
     if (!P) return SLCS_OK;
+    cudaFree(P->d_out16);
     for (auto &k : P->chunks) {
         slcs_batch_plan_destroy(k.plan);
         if (k.stream) cudaStreamDestroy(k.stream);

@@ -540,8 +540,7 @@ struct GlueArgs {
     const int32_t *child_res; // level l+1 results
     const int32_t *pmap;      // level l+1 maps
     const int32_t *qmap;
-    int32_t *C, *R;
-    uint8_t *H, *HC;
+    int32_t *CW, *RW;         // packed words: row r -> its column | hi << 31, column c -> its row | hi << 31
     int32_t *res;             // level l result
     int k, level;
     const int32_t *bad;
@@ -556,11 +555,9 @@ __global__ void __launch_bounds__(256) glue_kernel(GlueArgs A)
         node_of(i, A.level + 1, A.k, co, cs);
         const int prow = A.pmap[i];
         const int pcol = A.qmap[co + A.child_res[i]];
-        const uint8_t hi = co != po;
-        A.C[po + prow] = pcol;
-        A.H[po + prow] = hi;
-        A.R[po + pcol] = prow;
-        A.HC[po + pcol] = hi;
+        const int32_t hi = co != po ? INT_MIN : 0;
+        A.CW[po + prow] = pcol | hi;
+        A.RW[po + pcol] = prow | hi;
         A.res[po + prow] = pcol; // the union of both halves; the walk adds the fresh points
     }
 }
@@ -584,8 +581,7 @@ constexpr int WALK_GMAX = 1024; // grid lines per node and dimension, at most
 constexpr int WALK_BMIN = 64;   // smallest grid spacing
 
 struct TableArgs {
-    const int32_t *C;
-    const uint8_t *H;
+    const int32_t *__restrict__ CW; // row words (column | hi << 31)
     int32_t *cnt_hi; // (G+1)^2 per node, becomes the delta table
     int32_t *cnt_lo;
     int k, level, B, stride; // stride = Gmax+1 for the level
@@ -625,8 +621,9 @@ __global__ void __launch_bounds__(256) table_count_kernel(TableArgs A)
             }
         }
         const int G = s / A.B;
-        const int bi = min((i - o) / A.B, G), bj = min(A.C[i] / A.B, G);
-        int32_t *t = (A.H[i] ? A.cnt_hi : A.cnt_lo) + size_t(nd) * A.stride * A.stride;
+        const int32_t w = __ldg(A.CW + i);
+        const int bi = min((i - o) / A.B, G), bj = min((w & INT_MAX) / A.B, G);
+        int32_t *t = (w < 0 ? A.cnt_hi : A.cnt_lo) + size_t(nd) * A.stride * A.stride;
         atomicAdd(t + bi * A.stride + bj, 1);
     }
 }
@@ -717,10 +714,8 @@ __global__ void __launch_bounds__(1024) table_cols_kernel(TableArgs A, int nodes
 }
 
 struct SegArgs {
-    const int32_t *C;
-    const uint8_t *H;
-    const int32_t *R;
-    const uint8_t *HC;
+    const int32_t *__restrict__ CW; // row words (column | hi << 31)
+    const int32_t *__restrict__ RW; // column words (row | hi << 31)
     const int32_t *T; // delta tables
     int32_t *res;
     int k, level, B, stride, nseg; // nseg: segments per node
@@ -731,14 +726,12 @@ struct SegArgs {
 // leaves the lo count.
 __device__ __forceinline__ int rowinc(const SegArgs &A, int o, int r, int c)
 {
-    const int cc = A.C[o + r];
-    return A.H[o + r] ? (cc < c) : (cc >= c);
+    return word_inc(__ldg(A.CW + o + r), c);
 }
 // delta(r, c+1) - delta(r, c)
 __device__ __forceinline__ int colinc(const SegArgs &A, int o, int c, int r)
 {
-    const int rr = A.R[o + c];
-    return A.HC[o + c] ? (rr < r) : (rr >= r);
+    return word_inc(__ldg(A.RW + o + c), r);
 }
 
 __device__ __forceinline__ int warp_sum(int v)
@@ -754,7 +747,9 @@ __device__ int delta_at(const SegArgs &A, const int32_t *T, int o, int r, int c,
     const int i0 = r / A.B, j0 = c / A.B;
     const int r0 = i0 * A.B, c0 = j0 * A.B;
     int acc = 0;
+#pragma unroll 4
     for (int rr = r0 + lane; rr < r; rr += 32) acc += rowinc(A, o, rr, c0);
+#pragma unroll 4
     for (int cc = c0 + lane; cc < c; cc += 32) acc += colinc(A, o, cc, r);
     return T[i0 * A.stride + j0] + warp_sum(acc);
 }
@@ -789,7 +784,7 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
     if (E < e0) {
         dr = s - 1;
         dc = 0;
-        delta = A.H[o + s - 1] ? 0 : -1;
+        delta = __ldg(A.CW + o + s - 1) < 0 ? 0 : -1;
     } else {
         const int rlo = max(0, -E), rhi = min(s, s - E);
         if (rlo > rhi) return;
@@ -811,10 +806,16 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
             int dval = T[(istar - 1) * A.stride + (istar - 1) + jj];
             const int rend = min(istar * B, rhi);
             rstar = rhi + 1;
+            // The increments of the next 32 rows are loaded before this
+            // chunk is scanned, so that their latency overlaps the scan.
+            auto inc_at = [&](int r) {
+                return r < rend ? colinc(A, o, r + E, r) + rowinc(A, o, r, r + E + 1) : 0;
+            };
+            int inc_next = inc_at(rb + lane);
             for (; rb < rend; rb += 32) {
                 const int r = rb + lane;
-                int inc = 0;
-                if (r < rend) inc = colinc(A, o, r + E, r) + rowinc(A, o, r, r + E + 1);
+                const int inc = inc_next;
+                inc_next = inc_at(r + 32);
                 int pre = inc;
                 for (int off = 1; off < 32; off <<= 1) {
                     const int y = __shfl_up_sync(FULL_MASK, pre, off);
@@ -843,8 +844,10 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
     int32_t *wr_s = walk_smem + size_t(wi) * 2 * win, *wc_s = wr_s + win;
     const int rb = max(0, dr - B - 6), nr = min(max(dr - rb + 1, 0), win);
     const int cb = max(0, dc - 1), nc = min(max(min(s, dc + B + 6) - cb, 0), win);
-    for (int t = lane; t < nr; t += 32) wr_s[t] = A.C[o + rb + t] | (A.H[o + rb + t] ? INT_MIN : 0);
-    for (int t = lane; t < nc; t += 32) wc_s[t] = A.R[o + cb + t] | (A.HC[o + cb + t] ? INT_MIN : 0);
+#pragma unroll 4
+    for (int t = lane; t < nr; t += 32) wr_s[t] = __ldg(A.CW + o + rb + t);
+#pragma unroll 4
+    for (int t = lane; t < nc; t += 32) wc_s[t] = __ldg(A.RW + o + cb + t);
     __syncwarp();
     if (lane != 0) return;
     // Outside the window (B > WALK_WIN - 8 only) the walk reads global memory.
@@ -853,11 +856,11 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
         dr, dc, delta, s, E + B,
         [&](int r) {
             const unsigned t = unsigned(r - rb);
-            return t < unsigned(nr) ? wr[t] : (A.C[o + r] | (A.H[o + r] ? INT_MIN : 0));
+            return t < unsigned(nr) ? wr[t] : __ldg(A.CW + o + r);
         },
         [&](int c) {
             const unsigned t = unsigned(c - cb);
-            return t < unsigned(nc) ? wc[t] : (A.R[o + c] | (A.HC[o + c] ? INT_MIN : 0));
+            return t < unsigned(nc) ? wc[t] : __ldg(A.RW + o + c);
         },
         [&](int r, int c) { A.res[o + r] = c; });
 }
@@ -872,7 +875,9 @@ __device__ int delta_at_lane(const SegArgs &A, const int32_t *T, int o, int r, i
     const int i0 = r / A.B, j0 = c / A.B;
     const int r0 = i0 * A.B, c0 = j0 * A.B;
     int acc = T[i0 * A.stride + j0];
+#pragma unroll 4
     for (int rr = r0; rr < r; ++rr) acc += rowinc(A, o, rr, c0);
+#pragma unroll 4
     for (int cc = c0; cc < c; ++cc) acc += colinc(A, o, cc, r);
     return acc;
 }
@@ -896,7 +901,7 @@ __global__ void __launch_bounds__(256) walk_lanes_kernel(SegArgs A, int nodes)
     if (E < e0) {
         dr = s - 1;
         dc = 0;
-        delta = A.H[o + s - 1] ? 0 : -1;
+        delta = __ldg(A.CW + o + s - 1) < 0 ? 0 : -1;
     } else {
         const int rlo = max(0, -E), rhi = min(s, s - E);
         if (rlo > rhi) return;
@@ -927,8 +932,8 @@ __global__ void __launch_bounds__(256) walk_lanes_kernel(SegArgs A, int nodes)
         delta = delta_at_lane(A, T, o, dr, dc);
     }
     ant_walk(
-        dr, dc, delta, s, E + B, [&](int r) { return A.C[o + r] | (A.H[o + r] ? INT_MIN : 0); },
-        [&](int c) { return A.R[o + c] | (A.HC[o + c] ? INT_MIN : 0); }, [&](int r, int c) { A.res[o + r] = c; });
+        dr, dc, delta, s, E + B, [&](int r) { return __ldg(A.CW + o + r); },
+        [&](int c) { return __ldg(A.RW + o + c); }, [&](int r, int c) { A.res[o + r] = c; });
 }
 
 // ---------------------------------------------------------------------------
@@ -1163,7 +1168,7 @@ slcs_status braid_workspace_bytes(int p, int q, int k, int cutoff, size_t *bytes
     b += 4 * kk * sizeof(int32_t);                         // P/Q ping-pong
     b += 2 * kk * size_t(levels + 2) * sizeof(int32_t);    // maps per level
     b += kk * size_t(levels + 2) * sizeof(int32_t);        // results per level
-    b += 2 * kk * sizeof(int32_t) + 2 * kk;                // C, R, H, HC
+    b += 2 * kk * sizeof(int32_t);                         // row and column words
     b += 2 * size_t(std::max(n, k)) * sizeof(int32_t);     // scans
     b += 2 * (size_t(std::max(n, k)) / SCAN_BS + 2) * sizeof(int32_t);
     b += size_t(p) * sizeof(int32_t) + size_t(q) * sizeof(int32_t); // inverses
@@ -1204,8 +1209,6 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     int32_t *res = reinterpret_cast<int32_t *>(take(kk * size_t(levels + 2) * 4));
     int32_t *C = reinterpret_cast<int32_t *>(take(kk * 4));
     int32_t *Rr = reinterpret_cast<int32_t *>(take(kk * 4));
-    uint8_t *H = reinterpret_cast<uint8_t *>(take(kk));
-    uint8_t *HC = reinterpret_cast<uint8_t *>(take(kk));
     const size_t nscan = size_t(std::max(n, k));
     int32_t *scanP = reinterpret_cast<int32_t *>(take(nscan * 4));
     int32_t *scanQ = reinterpret_cast<int32_t *>(take(nscan * 4));
@@ -1275,7 +1278,7 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     // Levels above: glue, union, walk.
     for (int l = lc - 1; l >= 0; --l) {
         GlueArgs G{res + kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1) + kk,
-                   C, Rr, H, HC, res + kk * size_t(l), k, l, bad};
+                   C, Rr, res + kk * size_t(l), k, l, bad};
         glue_kernel<<<blocks_for(k, 256), 256, 0, st>>>(G);
         int B, stride;
         walk_grid(k, l, B, stride);
@@ -1284,7 +1287,7 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         // hi and lo counts of the level side by side: one clear for both
         int32_t *lvl_lo = tab_hi + tentries;
         SLCS_CUDA(cudaMemsetAsync(tab_hi, 0, 2 * tentries * sizeof(int32_t), st));
-        TableArgs TA{C, H, tab_hi, lvl_lo, k, l, B, stride, bad};
+        TableArgs TA{C, tab_hi, lvl_lo, k, l, B, stride, bad};
         table_count_kernel<<<blocks_for(k, 256), 256, 0, st>>>(TA);
         const int rows = nodes * stride;
         table_rows_kernel<<<int((long(rows) * 32 + 255) / 256), 256, 0, st>>>(TA, nodes);
@@ -1292,7 +1295,7 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         int smax = k;
         for (int d = 0; d < l; ++d) smax = smax - (smax >> 1);
         const int nseg = 2 * ((smax + B - 1) / B) + 2;
-        SegArgs SA{C, H, Rr, HC, tab_hi, res + kk * size_t(l), k, l, B, stride, nseg, bad};
+        SegArgs SA{C, Rr, tab_hi, res + kk * size_t(l), k, l, B, stride, nseg, bad};
         const long warps = long(nodes) * nseg;
         if (B <= WALK_LANE_B) {
             walk_lanes_kernel<<<int((warps + 255) / 256), 256, 0, st>>>(SA, nodes);

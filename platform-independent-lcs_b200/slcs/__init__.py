@@ -97,6 +97,7 @@ def lib():
         L.slcs_batch_plan_run.argtypes = [_vp, _vp, _vp, _vp, _vp]
         L.slcs_batch_plan_destroy.argtypes = [_vp]
         L.slcs_batch_plan_run_host.argtypes = [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp]
+        L.slcs_batch_plan_run_host16.argtypes = [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp]
         L.slcs_batch_plan_launches.argtypes = [_vp]
         L.slcs_batch_plan_launches.restype = _i32
         L.slcs_batch_plan_info.argtypes = [_vp, ctypes.POINTER(PlanInfo)]
@@ -293,6 +294,12 @@ class BatchPlan:
         h = torch.empty(len(self._descs), dtype=torch.int64, device=out.device)
         check(lib().slcs_batch_plan_hash(self._h, _dptr(out), _dptr(h), _stream(stream)))
         return h
+
+    def run_host16(self, a_blob: np.ndarray, b_blob: np.ndarray, out: np.ndarray, stream=None):
+        """As run_host with int16 strands in `out` (pairs with m + n <= 32767)."""
+        assert out.dtype == np.int16
+        check(lib().slcs_batch_plan_run_host16(self._h, a_blob.ctypes.data, a_blob.size, b_blob.ctypes.data,
+                                               b_blob.size, out.ctypes.data, out.size, _stream(stream)))
 
     def close(self):
         if self._h:

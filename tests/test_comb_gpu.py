@@ -400,3 +400,24 @@ def test_batch_run_host_chunked_ragged(cuda):
     plan.run_host(batch.a_blob, batch.b_blob, out)
     np.testing.assert_array_equal(out, _batch_expected(batch))
     plan.close()
+
+
+def test_batch_host_run_int16_strands(cuda):
+    """slcs_batch_plan_run_host16 returns the int32 run's strands as int16,
+    through the chunked path (20,000 reads) and the single-launch path (a
+    small batch); a plan with a pair of m + n > 32767 is refused."""
+    for batch in (W.reads_20000(), W.reads_20000(npairs=300, seed=9)):
+        _, total = batch.strand_offsets()
+        plan = slcs.BatchPlan(slcs.pair_descs(batch))
+        o32 = np.empty(total, np.int32)
+        o16 = np.full(total, -7, np.int16)
+        plan.run_host(batch.a_blob, batch.b_blob, o32)
+        plan.run_host16(batch.a_blob, batch.b_blob, o16)
+        assert np.array_equal(o16.astype(np.int32), o32)
+        plan.close()
+    big = W.pack([(np.zeros(20000, np.uint8), np.zeros(13000, np.uint8))])
+    plan = slcs.BatchPlan(slcs.pair_descs(big))
+    with pytest.raises(slcs.SlcsError) as err:
+        plan.run_host16(big.a_blob, big.b_blob, np.empty(33000, np.int16))
+    assert err.value.status == 6
+    plan.close()
