@@ -850,8 +850,19 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
     for (int t = lane; t < nc; t += 32) wc_s[t] = __ldg(A.RW + o + cb + t);
     __syncwarp();
     if (lane != 0) return;
-    // Outside the window (B > WALK_WIN - 8 only) the walk reads global memory.
     const int32_t *wr = wr_s, *wc = wc_s;
+    if (B + 12 <= WALK_WIN) {
+        // The window holds every row and column the walk reads (see above):
+        // shared memory only.  The index is clamped to the window, which
+        // changes nothing for the reads the walk makes and keeps any other
+        // inside the warp's own slice.
+        const unsigned rmax = unsigned(win - 1);
+        ant_walk(
+            dr, dc, delta, s, E + B, [&](int r) { return wr[min(unsigned(r - rb), rmax)]; },
+            [&](int c) { return wc[min(unsigned(c - cb), rmax)]; }, [&](int r, int c) { A.res[o + r] = c; });
+        return;
+    }
+    // Grids coarser than the window (k beyond 2^20): outside it, global memory.
     ant_walk(
         dr, dc, delta, s, E + B,
         [&](int r) {

@@ -122,3 +122,52 @@ def test_comb_pair_distributed_gloo(world, m, n, split):
         eh, ev = O.comb(a, b)
         np.testing.assert_array_equal(got["h"], eh)
         np.testing.assert_array_equal(got["v"], ev)
+
+
+def _worker_fail(rank, world, port, out_dir):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    try:
+        if rank == 1:
+            raise RuntimeError("rank 1 failed before its send")  # the failure, made on the host
+        rng = np.random.default_rng(3)
+        a = torch.from_numpy(rng.integers(0, 4, 200, dtype=np.uint8))
+        b = torch.from_numpy(rng.integers(0, 4, 500, dtype=np.uint8))
+        try:
+            D.comb_pair_distributed(a, b, kernels=OracleKernels(), split="strips")
+            open(os.path.join(out_dir, "rank0_finished"), "w").close()
+        except Exception as e:  # the receive from the failed rank ends in an error
+            with open(os.path.join(out_dir, "rank0_error"), "w") as f:
+                f.write(repr(e))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_failed_rank_ends_the_merge_with_an_error():
+    """A rank that fails before its send: the receiving rank's point-to-point
+    receive ends with an error (peer gone or the group's 10 s timeout)
+    instead of waiting for good; no GPU is involved."""
+    import socket
+    import time
+
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    with tempfile.TemporaryDirectory() as d:
+        ctx = mp.start_processes(_worker_fail, args=(2, port, d), nprocs=2, join=False, start_method="spawn")
+        deadline = time.time() + 120
+        for p in ctx.processes:
+            p.join(timeout=max(1.0, deadline - time.time()))
+        alive = [p for p in ctx.processes if p.is_alive()]
+        for p in alive:
+            p.kill()
+        assert not alive, "a rank was still waiting"
+        assert ctx.processes[1].exitcode != 0
+        assert os.path.exists(os.path.join(d, "rank0_error"))
+        assert not os.path.exists(os.path.join(d, "rank0_finished"))
