@@ -157,6 +157,18 @@ int auto_bands(int32_t m, int32_t n, int tm)
 
 } // namespace
 
+// Row bands of a pair combed as column strips (below 2^19 rows): a strip's
+// stripes form a chain that spends about 176 columns per stripe filling, so
+// from 2^16 rows on the strips are cut into bands of about 32768 rows (64
+// stripes of 16 rows per lane), at most 8.  Measured on B200, the 131072 x
+// 131072 mutated pair at 16 rows per lane and 4 strips: 1, 2, 4, 8 bands
+// 17.1, 14.4, 13.0, 14.0 ms; 2 x 8 and 8 x 4 tiles 13.8 and 14.7 ms.
+int strip_bands(int32_t m)
+{
+    if (m < (1 << 16)) return 1;
+    return std::min(8, std::max(1, int(m / 32768)));
+}
+
 // 14 or 16 rows per lane leave room for 8 warps per block; the smaller tiles run 4.
 int pick_warps(const slcs_config *cfg, int tm) { return (cfg && cfg->warps) ? cfg->warps : (tm >= 14 ? 8 : 4); }
 
@@ -188,8 +200,9 @@ slcs_status plan_pair(int32_t m, int32_t n, const slcs_config *cfg, int sms, Pai
     c.strips = 1;
     c.bands = 1;
     if (!auto_all) return SLCS_OK;
-    const int R = auto_bands(m, n, tm);
+    int R = auto_bands(m, n, tm);
     const int S = R > 1 ? 1 : auto_strips(m, n);
+    if (S > 1) R = strip_bands(m);
     if (R > 1 || S > 1) {
         c.algo = SLCS_ALGO_STRIPS;
         c.strips = S;

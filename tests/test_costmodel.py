@@ -69,7 +69,10 @@ def test_model_beats_fixed_heuristic_on_autotuner_timings(cuda):
     if not os.path.exists(DB):
         pytest.skip("no autotuner timing database committed")
     from slcs import autotune as AT
+    from slcs import costmodel as CM
     db = np.load(DB)
+    if list(db["variants"]) != [v["name"] for v in CM.VARIANTS]:
+        pytest.skip("the committed timings were taken for another variant list")
     model, loss = AT.fit(db["train_X"], db["train_ms"], epochs=1500)
     rep = AT.report(model, db["test_X"], db["test_ms"])
     assert rep["model"]["total_time_ratio"] < rep["heuristic"]["total_time_ratio"]

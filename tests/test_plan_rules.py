@@ -34,10 +34,12 @@ def test_narrow_tall_pair_takes_many_bands():
     assert p["cols_per_step"] == 4  # 74-stripe chains against 700 columns
 
 
-def test_mid_size_pairs_take_strips():
+def test_mid_size_pairs_take_strips_and_bands():
     p = plan(131072, 131072)
-    assert (p["algo"], p["tile_m"], p["warps"], p["strips"], p["bands"]) == (slcs.ALGO_STRIPS, 16, 4, 4, 1)
+    assert (p["algo"], p["tile_m"], p["warps"], p["strips"], p["bands"]) == (slcs.ALGO_STRIPS, 16, 4, 4, 4)
     assert p["cols_per_step"] == 4
+    assert plan(40000, 200000)["bands"] == 1  # below 2^16 rows: strips only
+    assert plan(70000, 300000)["bands"] == 2
 
 
 def test_small_pairs_stay_one_wavefront():
