@@ -11,16 +11,18 @@
 //     the node containing entry i at level l follows from i alone (node_of).
 //   * Downward, each level is a stable partition of every node: P's rows by
 //     column < s/2 (get_vert_slice, 5-19) and Q's columns by row < s/2
-//     (get_horz_slice, 22-36).  Above the cutoff the partition is a device-wide
-//     scan; the maps from child index to parent index are kept per level.
+//     (get_horz_slice, 22-36).  Above the cutoff the partition is one
+//     single-pass launch per level (tiles publish their counts and look back
+//     over their predecessors, every wait bounded); the maps from child index
+//     to parent index are kept per level.
 //   * A node at or below the cutoff is finished by one thread block: it loads
 //     the node into shared memory (16-bit local indices) and runs every lower
 //     level of its subtree there, down and back up, with block-wide scans.
 //   * Upward, a level scatters both children's products into the parent's
 //     rows and columns (inverse_mapping, 191-202) and, in the same pass, into
-//     the parent's result (the union of the two halves, 254-268); then it
-//     walks the ant (123-189) over every node, which writes the fresh points
-//     on top.
+//     the parent's result (the union of the two halves, 254-268) and into the
+//     block counts of the level's delta tables; then it walks the ant
+//     (123-189) over every node, which writes the fresh points on top.
 //   * Walks of small nodes run one thread per node.  A large node's walk is cut
 //     into segments that run concurrently: on every diagonal e = col - row the
 //     walk sits one row above r*(e-1), the first point of diagonal e-1 where
@@ -74,46 +76,7 @@ struct LevelArgs {
     const int32_t *bad;
 };
 
-__device__ __forceinline__ void flags_at(const LevelArgs &A, int i, int &fp, int &fq)
-{
-    int o, s;
-    node_of(i, A.level, A.k, o, s);
-    const int h = s >> 1;
-    fp = A.P[i] < h;
-    fq = A.Q[i] < h;
-}
 
-__global__ void __launch_bounds__(256) part_count_kernel(LevelArgs A)
-{
-    if (*A.bad) return;
-    const int base = blockIdx.x * SCAN_BS;
-    int cp = 0, cq = 0;
-    for (int i = base + threadIdx.x; i < min(base + SCAN_BS, A.k); i += blockDim.x) {
-        int fp, fq;
-        flags_at(A, i, fp, fq);
-        cp += fp;
-        cq += fq;
-    }
-    __shared__ int sp[8], sq[8];
-    for (int off = 16; off; off >>= 1) {
-        cp += __shfl_xor_sync(FULL_MASK, cp, off);
-        cq += __shfl_xor_sync(FULL_MASK, cq, off);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        sp[threadIdx.x >> 5] = cp;
-        sq[threadIdx.x >> 5] = cq;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int tp = 0, tq = 0;
-        for (int w = 0; w < 8; ++w) {
-            tp += sp[w];
-            tq += sq[w];
-        }
-        A.bsumP[blockIdx.x] = tp;
-        A.bsumQ[blockIdx.x] = tq;
-    }
-}
 
 // Exclusive scan of the block sums (one block; the count is k / SCAN_BS).
 __global__ void __launch_bounds__(1024) part_bsum_kernel(int32_t *bp, int32_t *bq, int nb)
@@ -167,46 +130,182 @@ __global__ void __launch_bounds__(1024) part_bsum_kernel(int32_t *bp, int32_t *b
     }
 }
 
-// Per block: exclusive scan of the flags in element order plus the block offset.
-__global__ void __launch_bounds__(256) part_scan_kernel(LevelArgs A)
+
+
+// ---------------------------------------------------------------------------
+// one level's partition in a single pass (count, scan and scatter fused)
+//
+// Tiles of SCAN_BS entries take tickets in launch order, so that a tile's
+// predecessors have all started.  A tile counts its flags, publishes the two
+// counts at once (AGG; tile 0 its inclusive prefix, INCL), then looks back
+// over its predecessors -- adding AGG counts until it meets a tile that
+// published INCL -- and publishes its own INCL.  It then writes its exclusive
+// scan values and raises its `done` flag after them.  The scatter of an
+// entry needs the scan value at its node's first entry; when that entry lies
+// in an earlier tile, the tile waits for that tile's `done` (INCL alone is
+// published before the scan values are written).  A tile waits only on
+// words its predecessors publish without waiting themselves, or on `done`,
+// which follows a look-back over such words, so every wait ends; each is
+// also bounded by %globaltimer, and one that runs out raises the product's
+// error flag (every later kernel returns early) and DEV_ERR_TIMEOUT.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long TILE_AGG = 1ull << 62, TILE_INCL = 2ull << 62;
+constexpr unsigned long long TILE_COUNT_MASK = (1ull << 31) - 1;
+constexpr uint64_t PART_WAIT_NS = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
 {
-    if (*A.bad) return;
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long pack_counts(unsigned long long flag, int cp, int cq)
+{
+    return flag | (unsigned long long)(unsigned(cp)) | ((unsigned long long)(unsigned(cq)) << 31);
+}
+
+struct FusedArgs {
+    LevelArgs L;
+    unsigned long long *tiles; // status word per tile of this level, zero at launch
+    int32_t *done;             // per tile of this level: scan values written (1), zero at launch
+    int32_t *ticket;           // tile ticket of this level, zero at launch
+    int32_t *err;              // the product's error flag
+    uint32_t *status;          // device status word
+};
+
+// Thread 0: spin until *p has one of `want` flags, bounded; 0 on expiry.
+__device__ __forceinline__ unsigned long long wait_tile(const FusedArgs &F, const unsigned long long *p,
+                                                        unsigned long long want)
+{
+    uint64_t t0 = 0;
+    for (;;) {
+        const unsigned long long v = ld_acquire_u64(p);
+        if (v & want) return v;
+        if (ld_relaxed_gpu(F.err)) return 0;
+        const uint64_t now = globaltimer_ns();
+        if (t0 == 0) {
+            t0 = now;
+        } else if (now - t0 > PART_WAIT_NS) {
+            atomicExch(F.err, 1);
+            raise_status(F.status, DEV_ERR_TIMEOUT);
+            return 0;
+        }
+        __nanosleep(64);
+    }
+}
+
+// Thread 0: spin until done[t] is set, bounded; false on expiry.
+__device__ __forceinline__ bool wait_done(const FusedArgs &F, int t)
+{
+    uint64_t t0 = 0;
+    for (;;) {
+        if (ld_acquire_gpu(F.done + t)) return true;
+        if (ld_relaxed_gpu(F.err)) return false;
+        const uint64_t now = globaltimer_ns();
+        if (t0 == 0) {
+            t0 = now;
+        } else if (now - t0 > PART_WAIT_NS) {
+            atomicExch(F.err, 1);
+            raise_status(F.status, DEV_ERR_TIMEOUT);
+            return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+__global__ void __launch_bounds__(256) part_fused_kernel(FusedArgs F)
+{
+    const LevelArgs &A = F.L;
+    __shared__ int s_tile, s_ok;
+    __shared__ int wp[8], wq[8];
+    __shared__ int s_ep, s_eq; // exclusive prefix of the tile
+    if (threadIdx.x == 0) {
+        s_tile = atomicAdd(F.ticket, 1);
+        s_ok = !ld_relaxed_gpu(F.err);
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    const int tile = s_tile;
     constexpr int PER = SCAN_BS / 256;
-    const int base = blockIdx.x * SCAN_BS + threadIdx.x * PER;
+    const int base = tile * SCAN_BS + threadIdx.x * PER;
+    // Each entry's node, values and flags, kept for the scatter.
+    int eo[PER], es[PER], ep_[PER], eq_[PER];
     int fp[PER], fq[PER];
     int cp = 0, cq = 0;
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         const int i = base + j;
-        if (i < A.k) flags_at(A, i, fp[j], fq[j]);
-        else fp[j] = fq[j] = 0;
+        eo[j] = es[j] = ep_[j] = eq_[j] = 0;
+        fp[j] = fq[j] = 0;
+        if (i < A.k) {
+            node_of(i, A.level, A.k, eo[j], es[j]);
+            ep_[j] = A.P[i];
+            eq_[j] = A.Q[i];
+            const int h = es[j] >> 1;
+            fp[j] = ep_[j] < h;
+            fq[j] = eq_[j] < h;
+        }
         cp += fp[j];
         cq += fq[j];
     }
     int xp = cp, xq = cq;
     for (int off = 1; off < 32; off <<= 1) {
-        int yp = __shfl_up_sync(FULL_MASK, xp, off), yq = __shfl_up_sync(FULL_MASK, xq, off);
+        const int yp = __shfl_up_sync(FULL_MASK, xp, off), yq = __shfl_up_sync(FULL_MASK, xq, off);
         if ((threadIdx.x & 31) >= off) {
             xp += yp;
             xq += yq;
         }
     }
-    __shared__ int wp[8], wq[8];
     if ((threadIdx.x & 31) == 31) {
         wp[threadIdx.x >> 5] = xp;
         wq[threadIdx.x >> 5] = xq;
     }
     __syncthreads();
-    int op = A.bsumP[blockIdx.x], oq = A.bsumQ[blockIdx.x];
+    if (threadIdx.x == 0) {
+        int tp = 0, tq = 0;
+        for (int w = 0; w < 8; ++w) {
+            tp += wp[w];
+            tq += wq[w];
+        }
+        int ep = 0, eq = 0;
+        if (tile == 0) {
+            st_release_u64(F.tiles, pack_counts(TILE_INCL, tp, tq));
+        } else {
+            st_release_u64(F.tiles + tile, pack_counts(TILE_AGG, tp, tq));
+            for (int j = tile - 1; j >= 0; --j) {
+                const unsigned long long v = wait_tile(F, F.tiles + j, TILE_AGG | TILE_INCL);
+                if (!v) {
+                    s_ok = 0;
+                    break;
+                }
+                ep += int(v & TILE_COUNT_MASK);
+                eq += int((v >> 31) & TILE_COUNT_MASK);
+                if (v & TILE_INCL) break;
+            }
+            if (s_ok) st_release_u64(F.tiles + tile, pack_counts(TILE_INCL, ep + tp, eq + tq));
+        }
+        s_ep = ep;
+        s_eq = eq;
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    int op = s_ep, oq = s_eq;
     for (int w = 0; w < (threadIdx.x >> 5); ++w) {
         op += wp[w];
         oq += wq[w];
     }
     op += xp - cp;
     oq += xq - cq;
+    int sp[PER], sq[PER];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         const int i = base + j;
+        sp[j] = op;
+        sq[j] = oq;
         if (i < A.k) {
             A.scanP[i] = op;
             A.scanQ[i] = oq;
@@ -214,21 +313,46 @@ __global__ void __launch_bounds__(256) part_scan_kernel(LevelArgs A)
         op += fp[j];
         oq += fq[j];
     }
-}
-
-__global__ void __launch_bounds__(256) part_scatter_kernel(LevelArgs A)
-{
-    if (*A.bad) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.k; i += gridDim.x * blockDim.x) {
-        int o, s;
-        node_of(i, A.level, A.k, o, s);
-        const int h = s >> 1;
-        const int p = A.P[i], q = A.Q[i];
-        const int bp = A.scanP[i] - A.scanP[o];
-        const int bq = A.scanQ[i] - A.scanQ[o];
+    __threadfence();
+    __syncthreads();
+    // This tile's scan values are written; then make sure those of the tile
+    // holding the node start of the tile's first entry are too.
+    if (threadIdx.x == 0) {
+        st_release_gpu(F.done + tile, 1);
+        int o, sz;
+        node_of(tile * SCAN_BS, A.level, A.k, o, sz);
+        const int t_o = o / SCAN_BS;
+        if (t_o < tile && !wait_done(F, t_o)) s_ok = 0;
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    // Scan values at the node starts: written before the barrier above (this
+    // tile) or before a done flag thread 0 acquired (an earlier tile); read
+    // through L2, the point of coherence, in one batch.
+    int so_p[PER], so_q[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        so_p[j] = base + j < A.k ? __ldcg(A.scanP + eo[j]) : 0;
+        so_q[j] = base + j < A.k ? __ldcg(A.scanQ + eo[j]) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        const int i = base + j;
+        if (i >= A.k) break;
+        const int o = eo[j], sz = es[j];
+        const int h = sz >> 1;
+        const int p = ep_[j], q = eq_[j];
+        const int bp = sp[j] - so_p[j], bq = sq[j] - so_q[j];
         const int local = i - o;
         const int pp = p < h ? o + bp : o + h + (local - bp);
         const int pq = q < h ? o + bq : o + h + (local - bq);
+        // A destination outside the node can only come from a wrong scan
+        // value: report it and store nothing.
+        if (unsigned(pp - o) >= unsigned(sz) || unsigned(pq - o) >= unsigned(sz)) {
+            atomicExch(F.err, 1);
+            raise_status(F.status, DEV_ERR_BOUNDS);
+            continue;
+        }
         A.Pn[pp] = p < h ? p : p - h;
         A.pmap[pp] = local;
         A.Qn[pq] = q < h ? q : q - h;
@@ -544,21 +668,42 @@ struct GlueArgs {
     int32_t *res;             // level l result
     int k, level;
     const int32_t *bad;
+    // Block counts of the level's delta tables, counted as the points are
+    // glued: (G+1)^2 per node and table, G = node size / B.
+    int32_t *cnt_hi, *cnt_lo;
+    int B, stride;
 };
 
 __global__ void __launch_bounds__(256) glue_kernel(GlueArgs A)
 {
     if (*A.bad) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.k; i += gridDim.x * blockDim.x) {
-        int po, ps, co, cs;
-        node_of(i, A.level, A.k, po, ps);
-        node_of(i, A.level + 1, A.k, co, cs);
+        // parent node (offset, size, index) and child node of entry i
+        int po = 0, ps = A.k, nd = 0;
+        for (int d = 0; d < A.level; ++d) {
+            const int h = ps >> 1;
+            nd <<= 1;
+            if (i < po + h) {
+                ps = h;
+            } else {
+                po += h;
+                ps -= h;
+                nd |= 1;
+            }
+        }
+        const int co = i < po + (ps >> 1) ? po : po + (ps >> 1);
         const int prow = A.pmap[i];
         const int pcol = A.qmap[co + A.child_res[i]];
         const int32_t hi = co != po ? INT_MIN : 0;
         A.CW[po + prow] = pcol | hi;
         A.RW[po + pcol] = prow | hi;
         A.res[po + prow] = pcol; // the union of both halves; the walk adds the fresh points
+        if (A.cnt_hi) {
+            const int G = ps / A.B;
+            const int bi = min(prow / A.B, G), bj = min(pcol / A.B, G);
+            int32_t *t = (hi ? A.cnt_hi : A.cnt_lo) + size_t(nd) * A.stride * A.stride;
+            atomicAdd(t + bi * A.stride + bj, 1);
+        }
     }
 }
 
@@ -600,31 +745,6 @@ __device__ __forceinline__ void node_by_index(int nd, int level, int k, int &o, 
         } else {
             s = h;
         }
-    }
-}
-
-__global__ void __launch_bounds__(256) table_count_kernel(TableArgs A)
-{
-    if (*A.bad) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.k; i += gridDim.x * blockDim.x) {
-        // node and its index (the path of hi/lo choices)
-        int o = 0, s = A.k, nd = 0;
-        for (int d = 0; d < A.level; ++d) {
-            const int h = s >> 1;
-            nd <<= 1;
-            if (i < o + h) {
-                s = h;
-            } else {
-                o += h;
-                s -= h;
-                nd |= 1;
-            }
-        }
-        const int G = s / A.B;
-        const int32_t w = __ldg(A.CW + i);
-        const int bi = min((i - o) / A.B, G), bj = min((w & INT_MAX) / A.B, G);
-        int32_t *t = (w < 0 ? A.cnt_hi : A.cnt_lo) + size_t(nd) * A.stride * A.stride;
-        atomicAdd(t + bi * A.stride + bj, 1);
     }
 }
 
@@ -688,11 +808,13 @@ __global__ void __launch_bounds__(1024) table_cols_kernel(TableArgs A, int nodes
     int32_t *lo = A.cnt_lo + size_t(nd) * A.stride * A.stride + j;
     __shared__ int Hs[32][33], Ls[32][33];
     int hs = 0, ls = 0;
-    if (col_ok)
+    if (col_ok) {
+#pragma unroll 8
         for (int i = i0; i < i1; ++i) {
             hs += hi[size_t(i) * A.stride];
             ls += lo[size_t(i) * A.stride];
         }
+    }
     Hs[ty][tx] = hs;
     Ls[ty][tx] = ls;
     __syncthreads();
@@ -701,15 +823,65 @@ __global__ void __launch_bounds__(1024) table_cols_kernel(TableArgs A, int nodes
     for (int t = ty + 1; t < 32; ++t) loff += Ls[t][tx];
     if (!col_ok) return;
     int run = loff;
+#pragma unroll 4
     for (int i = i1 - 1; i >= i0; --i) {
         run += lo[size_t(i) * A.stride];
         lo[size_t(i) * A.stride] = run; // #lo points with row >= iB, col >= jB
     }
     run = hoff;
+#pragma unroll 4
     for (int i = i0; i < i1; ++i) {
         const int v = hi[size_t(i) * A.stride];
         hi[size_t(i) * A.stride] = run - lo[size_t(i) * A.stride]; // delta(iB, jB)
         run += v;
+    }
+}
+
+// Levels whose tables have at most SMALL_TABLE entries: one block per node
+// finishes the whole table in shared memory (row pass, then column pass):
+// delta(iB, jB) = #{hi blocks above-left} - #{lo blocks at or below-right}.
+constexpr int SMALL_TABLE = 4096;
+__global__ void __launch_bounds__(256) table_small_kernel(TableArgs A, int nodes)
+{
+    if (*A.bad) return;
+    __shared__ int32_t hs[SMALL_TABLE], ls[SMALL_TABLE];
+    const int nd = blockIdx.x;
+    if (nd >= nodes) return;
+    int o, s;
+    node_by_index(nd, A.level, A.k, o, s);
+    const int G = s / A.B, W = A.stride, n = (G + 1) * W;
+    int32_t *hi = A.cnt_hi + size_t(nd) * W * W, *lo = A.cnt_lo + size_t(nd) * W * W;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        hs[t] = hi[t];
+        ls[t] = lo[t];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= G; i += blockDim.x) { // rows: hi exclusive prefix, lo inclusive suffix
+        int run = 0;
+        for (int j = 0; j <= G; ++j) {
+            const int v = hs[i * W + j];
+            hs[i * W + j] = run;
+            run += v;
+        }
+        run = 0;
+        for (int j = G; j >= 0; --j) {
+            run += ls[i * W + j];
+            ls[i * W + j] = run;
+        }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j <= G; j += blockDim.x) { // columns, then delta into the hi table
+        int run = 0;
+        for (int i = G; i >= 0; --i) {
+            run += ls[i * W + j];
+            ls[i * W + j] = run;
+        }
+        run = 0;
+        for (int i = 0; i <= G; ++i) {
+            const int v = hs[i * W + j];
+            hi[i * W + j] = run - ls[i * W + j];
+            run += v;
+        }
     }
 }
 
@@ -1185,6 +1357,7 @@ slcs_status braid_workspace_bytes(int p, int q, int k, int cutoff, size_t *bytes
     b += size_t(p) * sizeof(int32_t) + size_t(q) * sizeof(int32_t); // inverses
     b += 2 * kk * sizeof(int32_t);                         // map_row, map_col
     b += 64 * 256 + 256;                                    // alignment slack, flag
+    b += size_t(levels + 1) * ((size_t(std::max(k, 1)) + SCAN_BS - 1) / SCAN_BS) * 12 + 512; // partition tiles
     *bytes = b;
     return SLCS_OK;
 }
@@ -1230,12 +1403,23 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     int32_t *Q_c2r = reinterpret_cast<int32_t *>(take(size_t(q) * 4));
     int32_t *map_row = reinterpret_cast<int32_t *>(take(kk * 4));
     int32_t *map_col = reinterpret_cast<int32_t *>(take(kk * 4));
-    int32_t *bad = reinterpret_cast<int32_t *>(take(256));
+    // Error flag, then the fused partitions' tile words (one per tile and
+    // level), their done flags and tickets (one per level): zeroed by one
+    // memset.
+    const int lc = cutoff_level(k, cutoff); // first level whose nodes fit a block
+    const int kb = int((kk + SCAN_BS - 1) / SCAN_BS);
+    const size_t tile_words = size_t(lc) * size_t(kb);
+    const size_t sync_bytes = 256 + tile_words * 8 + tile_words * 4 + 256;
+    char *sync_area = take(sync_bytes);
+    int32_t *bad = reinterpret_cast<int32_t *>(sync_area);
+    unsigned long long *tiles = reinterpret_cast<unsigned long long *>(sync_area + 256);
+    int32_t *done = reinterpret_cast<int32_t *>(sync_area + 256 + tile_words * 8);
+    int32_t *tickets = reinterpret_cast<int32_t *>(sync_area + 256 + tile_words * 12);
     const size_t tints = table_ints(k, cutoff);
     int32_t *tab_hi = reinterpret_cast<int32_t *>(take(2 * tints * 4)); // hi then lo counts of a level
     if (size_t(cur - static_cast<char *>(ws)) > ws_bytes) return fail(SLCS_ERR_ALLOC, "braid workspace too small");
 
-    SLCS_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), st));
+    SLCS_CUDA(cudaMemsetAsync(sync_area, 0, sync_bytes, st));
     SLCS_CUDA(cudaMemsetAsync(P_c2r, 0xff, size_t(p) * 4, st));
     SLCS_CUDA(cudaMemsetAsync(Q_c2r, 0xff, size_t(q) * 4, st));
     inverse_kernel<<<blocks_for(p, 256), 256, 0, st>>>(P, P_c2r, p, bad);
@@ -1250,16 +1434,13 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         part_bsum_kernel<<<1, 1024, 0, st>>>(bsP, bsQ, nbs);
         slice_write_kernel<<<nbs, 256, 0, st>>>(S);
     }
-    // Levels above the cutoff: device-wide partitions.
-    const int lc = cutoff_level(k, cutoff); // first level whose nodes fit a block
-    const int kb = int((kk + SCAN_BS - 1) / SCAN_BS);
+    // Levels above the cutoff: device-wide partitions, one fused launch each.
     for (int l = 0; l < lc; ++l) {
         LevelArgs A{Pcur, Qcur, Pnext, Qnext, maps + 2 * kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1) + kk,
                     scanP, scanQ, bsP, bsQ, k, l, bad};
-        part_count_kernel<<<kb, 256, 0, st>>>(A);
-        part_bsum_kernel<<<1, 1024, 0, st>>>(bsP, bsQ, kb);
-        part_scan_kernel<<<kb, 256, 0, st>>>(A);
-        part_scatter_kernel<<<blocks_for(k, 256), 256, 0, st>>>(A);
+        FusedArgs F{A, tiles + size_t(l) * size_t(kb), done + size_t(l) * size_t(kb), tickets + l, bad,
+                    device_status_word()};
+        part_fused_kernel<<<kb, 256, 0, st>>>(F);
         std::swap(Pcur, Pnext);
         std::swap(Qcur, Qnext);
     }
@@ -1288,21 +1469,25 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     }
     // Levels above: glue, union, walk.
     for (int l = lc - 1; l >= 0; --l) {
-        GlueArgs G{res + kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1) + kk,
-                   C, Rr, res + kk * size_t(l), k, l, bad};
-        glue_kernel<<<blocks_for(k, 256), 256, 0, st>>>(G);
         int B, stride;
         walk_grid(k, l, B, stride);
         const int nodes = 1 << l;
         const size_t tentries = size_t(nodes) * stride * stride;
-        // hi and lo counts of the level side by side: one clear for both
+        // hi and lo counts of the level side by side: one clear for both,
+        // filled by the glue as it places the points
         int32_t *lvl_lo = tab_hi + tentries;
         SLCS_CUDA(cudaMemsetAsync(tab_hi, 0, 2 * tentries * sizeof(int32_t), st));
+        GlueArgs G{res + kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1) + kk,
+                   C, Rr, res + kk * size_t(l), k, l, bad, tab_hi, lvl_lo, B, stride};
+        glue_kernel<<<blocks_for(k, 256), 256, 0, st>>>(G);
         TableArgs TA{C, tab_hi, lvl_lo, k, l, B, stride, bad};
-        table_count_kernel<<<blocks_for(k, 256), 256, 0, st>>>(TA);
-        const int rows = nodes * stride;
-        table_rows_kernel<<<int((long(rows) * 32 + 255) / 256), 256, 0, st>>>(TA, nodes);
-        table_cols_kernel<<<nodes * ((stride + 31) / 32), 1024, 0, st>>>(TA, nodes);
+        if (size_t(stride) * stride <= size_t(SMALL_TABLE)) {
+            table_small_kernel<<<nodes, 256, 0, st>>>(TA, nodes);
+        } else {
+            const int rows = nodes * stride;
+            table_rows_kernel<<<int((long(rows) * 32 + 255) / 256), 256, 0, st>>>(TA, nodes);
+            table_cols_kernel<<<nodes * ((stride + 31) / 32), 1024, 0, st>>>(TA, nodes);
+        }
         int smax = k;
         for (int d = 0; d < l; ++d) smax = smax - (smax >> 1);
         const int nseg = 2 * ((smax + B - 1) / B) + 2;
