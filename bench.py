@@ -273,6 +273,8 @@ def main():
     from slcs import distributed as D
     from slcs import tuning
 
+    if world > 1:
+        print(f"bench.py: rank {rank} of {world} (local rank {local})", file=sys.stderr, flush=True)
     if not torch.cuda.is_available():
         print("bench.py: the GPU arm needs a CUDA device", file=sys.stderr)
         return 2

@@ -37,3 +37,28 @@ def test_reference_arm_json_line():
     e = d["e2e"]
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+
+
+def test_gpus_flag_starts_one_rank_per_gpu():
+    """--gpus 2 without a torchrun environment starts two ranks of bench.py
+    (torch.distributed.run on 127.0.0.1); on a machine without a GPU each
+    rank then stops at the device check, so the launcher reports failure."""
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    env["CUDA_VISIBLE_DEVICES"] = ""
+    r = subprocess.run([sys.executable, "bench.py", "--gpus", "2", "--steps", "1", "--warmup", "1"], cwd=ROOT,
+                       capture_output=True, text=True, timeout=300, env=env)
+    out = r.stdout + r.stderr
+    # the first rank to stop makes the launcher end the other, so one
+    # announcement is certain and the launcher's summary names both ranks
+    assert "of 2 (local rank" in out, out[-2000:]
+    assert "rank 1 of 2" in out or "local_rank: 1" in out
+    assert "rank 0 of 2" in out or "local_rank: 0" in out
+    assert "needs a CUDA device" in out
+    assert r.returncode != 0
+
+
+def test_world_size_must_match_gpus():
+    env = dict(os.environ, WORLD_SIZE="3", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, "bench.py", "--gpus", "2", "--steps", "1", "--warmup", "1"], cwd=ROOT,
+                       capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 2 and "WORLD_SIZE 3" in r.stderr
