@@ -90,7 +90,7 @@ class ClockSampler:
                         self.reasons.add(name)
             except Exception:
                 pass
-            time.sleep(0.005)
+            time.sleep(0.001)  # the 20-step timed region lasts about 8 ms
 
     def __enter__(self):
         if self.ok:
