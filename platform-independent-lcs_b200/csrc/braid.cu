@@ -137,9 +137,9 @@ __global__ void __launch_bounds__(1024) part_bsum_kernel(int32_t *bp, int32_t *b
 //
 // Tiles of SCAN_BS entries take tickets in launch order, so that a tile's
 // predecessors have all started.  A tile counts its flags, publishes the two
-// counts at once (AGG; tile 0 its inclusive prefix, INCL), then looks back
-// over its predecessors -- adding AGG counts until it meets a tile that
-// published INCL -- and publishes its own INCL.  It then writes its exclusive
+// counts at once (AGG; tile 0 its inclusive prefix, INCL), then one warp
+// looks back over its predecessors 32 at a time -- adding AGG counts until
+// it meets a tile that published INCL -- and publishes its own INCL.  It then writes its exclusive
 // scan values and raises its `done` flag after them.  The scatter of an
 // entry needs the scan value at its node's first entry; when that entry lies
 // in an earlier tile, the tile waits for that tile's `done` (INCL alone is
@@ -176,27 +176,6 @@ struct FusedArgs {
     int32_t *err;              // the product's error flag
     uint32_t *status;          // device status word
 };
-
-// Thread 0: spin until *p has one of `want` flags, bounded; 0 on expiry.
-__device__ __forceinline__ unsigned long long wait_tile(const FusedArgs &F, const unsigned long long *p,
-                                                        unsigned long long want)
-{
-    uint64_t t0 = 0;
-    for (;;) {
-        const unsigned long long v = ld_acquire_u64(p);
-        if (v & want) return v;
-        if (ld_relaxed_gpu(F.err)) return 0;
-        const uint64_t now = globaltimer_ns();
-        if (t0 == 0) {
-            t0 = now;
-        } else if (now - t0 > PART_WAIT_NS) {
-            atomicExch(F.err, 1);
-            raise_status(F.status, DEV_ERR_TIMEOUT);
-            return 0;
-        }
-        __nanosleep(64);
-    }
-}
 
 // Thread 0: spin until done[t] is set, bounded; false on expiry.
 __device__ __forceinline__ bool wait_done(const FusedArgs &F, int t)
@@ -265,31 +244,71 @@ __global__ void __launch_bounds__(256) part_fused_kernel(FusedArgs F)
         wq[threadIdx.x >> 5] = xq;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    // Warp 0 publishes the tile's counts and looks back over its
+    // predecessors 32 at a time: lane l reads tile (front - 1 - l); the
+    // window's nearest INCL ends the look-back, otherwise its 32 AGG counts
+    // are added and the window moves back.  A window with a tile that has
+    // not published yet is read again (bounded by %globaltimer).
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
         int tp = 0, tq = 0;
         for (int w = 0; w < 8; ++w) {
             tp += wp[w];
             tq += wq[w];
         }
         int ep = 0, eq = 0;
+        bool ok = true;
         if (tile == 0) {
-            st_release_u64(F.tiles, pack_counts(TILE_INCL, tp, tq));
+            if (lane == 0) st_release_u64(F.tiles, pack_counts(TILE_INCL, tp, tq));
         } else {
-            st_release_u64(F.tiles + tile, pack_counts(TILE_AGG, tp, tq));
-            for (int j = tile - 1; j >= 0; --j) {
-                const unsigned long long v = wait_tile(F, F.tiles + j, TILE_AGG | TILE_INCL);
-                if (!v) {
-                    s_ok = 0;
-                    break;
+            if (lane == 0) st_release_u64(F.tiles + tile, pack_counts(TILE_AGG, tp, tq));
+            int front = tile; // the window covers tiles [front - 32, front)
+            uint64_t t0 = 0;
+            while (front > 0) {
+                const int j = front - 1 - lane;
+                const unsigned long long v = j >= 0 ? ld_acquire_u64(F.tiles + j) : TILE_INCL;
+                if (__any_sync(FULL_MASK, (v & (TILE_AGG | TILE_INCL)) == 0)) {
+                    // a predecessor has not counted yet: read the window again
+                    int stop = 0;
+                    if (lane == 0) {
+                        const uint64_t now = globaltimer_ns();
+                        if (ld_relaxed_gpu(F.err)) {
+                            stop = 1;
+                        } else if (t0 == 0) {
+                            t0 = now;
+                        } else if (now - t0 > PART_WAIT_NS) {
+                            atomicExch(F.err, 1);
+                            raise_status(F.status, DEV_ERR_TIMEOUT);
+                            stop = 1;
+                        }
+                    }
+                    if (__shfl_sync(FULL_MASK, stop, 0)) {
+                        ok = false;
+                        break;
+                    }
+                    __nanosleep(64);
+                    continue;
                 }
-                ep += int(v & TILE_COUNT_MASK);
-                eq += int((v >> 31) & TILE_COUNT_MASK);
-                if (v & TILE_INCL) break;
+                const unsigned incl = __ballot_sync(FULL_MASK, (v & TILE_INCL) != 0);
+                const int first = incl ? __ffs(incl) - 1 : 32; // nearest INCL in the window
+                int cp_ = lane <= first && j >= 0 ? int(v & TILE_COUNT_MASK) : 0;
+                int cq_ = lane <= first && j >= 0 ? int((v >> 31) & TILE_COUNT_MASK) : 0;
+                for (int off = 16; off; off >>= 1) {
+                    cp_ += __shfl_xor_sync(FULL_MASK, cp_, off);
+                    cq_ += __shfl_xor_sync(FULL_MASK, cq_, off);
+                }
+                ep += cp_;
+                eq += cq_;
+                if (incl) break;
+                front -= 32;
             }
-            if (s_ok) st_release_u64(F.tiles + tile, pack_counts(TILE_INCL, ep + tp, eq + tq));
+            if (ok && lane == 0) st_release_u64(F.tiles + tile, pack_counts(TILE_INCL, ep + tp, eq + tq));
         }
-        s_ep = ep;
-        s_eq = eq;
+        if (lane == 0) {
+            if (!ok) s_ok = 0;
+            s_ep = ep;
+            s_eq = eq;
+        }
     }
     __syncthreads();
     if (!s_ok) return;
