@@ -41,6 +41,11 @@ namespace slcs {
 namespace {
 
 constexpr int SCAN_BS = 2048;   // elements per block of the device-wide scan
+constexpr int PART_PER = 8;     // entries per thread of a partition tile
+// Threads of a partition tile: 1024 (8192 entries, one tile per SM at a time,
+// a short look-back chain) for large products, 256 (2048 entries) below.
+constexpr int PART_BIG_K = 1 << 19;
+__host__ __device__ constexpr int part_threads(int k) { return k >= PART_BIG_K ? 1024 : 256; }
 constexpr int SUB_THREADS = 512; // threads of the subtree block
 constexpr int SUB_MAX = 4096;   // largest node a block finishes in shared memory
 // Shared memory of a subtree block for nodes of up to maxn entries: two int32
@@ -135,7 +140,7 @@ __global__ void __launch_bounds__(1024) part_bsum_kernel(int32_t *bp, int32_t *b
 // ---------------------------------------------------------------------------
 // one level's partition in a single pass (count, scan and scatter fused)
 //
-// Tiles of SCAN_BS entries take tickets in launch order, so that a tile's
+// Tiles of THREADS * PART_PER entries take tickets in launch order, so that a tile's
 // predecessors have all started.  A tile counts its flags, publishes the two
 // counts at once (AGG; tile 0 its inclusive prefix, INCL), then one warp
 // looks back over its predecessors 32 at a time -- adding AGG counts until
@@ -196,12 +201,18 @@ __device__ __forceinline__ bool wait_done(const FusedArgs &F, int t)
     }
 }
 
-__global__ void __launch_bounds__(256) part_fused_kernel(FusedArgs F)
+template <int PART_THREADS>
+__global__ void __launch_bounds__(PART_THREADS) part_fused_kernel(FusedArgs F)
 {
     const LevelArgs &A = F.L;
+    constexpr int PER = PART_PER;
+    constexpr int PART_BS = PART_THREADS * PART_PER;
+    constexpr int WARPS = PART_THREADS / 32;
+    constexpr int GROUPS = PER * WARPS;         // runs of 32 entries per tile
+    constexpr int GPL = GROUPS / 32;            // groups per lane of the scanning warp
     __shared__ int s_tile, s_ok;
-    __shared__ int wp[8], wq[8];
-    __shared__ int s_ep, s_eq; // exclusive prefix of the tile
+    __shared__ int gp[GROUPS], gq[GROUPS]; // group counts, then their exclusive prefixes in the tile
+    __shared__ int s_ep, s_eq;             // exclusive prefix of the tile
     if (threadIdx.x == 0) {
         s_tile = atomicAdd(F.ticket, 1);
         s_ok = !ld_relaxed_gpu(F.err);
@@ -209,52 +220,67 @@ __global__ void __launch_bounds__(256) part_fused_kernel(FusedArgs F)
     __syncthreads();
     if (!s_ok) return;
     const int tile = s_tile;
-    constexpr int PER = SCAN_BS / 256;
-    const int base = tile * SCAN_BS + threadIdx.x * PER;
-    // Each entry's node, values and flags, kept for the scatter.
-    int eo[PER], es[PER], ep_[PER], eq_[PER];
-    int fp[PER], fq[PER];
-    int cp = 0, cq = 0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    // Striped: entry j of the thread is tile entry j * PART_THREADS +
+    // threadIdx.x, so that group g = j * WARPS + w is a run of 32 consecutive
+    // entries, loaded and stored by one warp instruction each.  A flag's rank
+    // inside its group comes from a ballot; the flags stay in two bit masks
+    // and the entries' values are read again for the scatter.
+    const int base = tile * PART_BS + threadIdx.x;
+    int eo[PER], es[PER];
+    unsigned fbits = 0, gbits = 0;
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-        const int i = base + j;
-        eo[j] = es[j] = ep_[j] = eq_[j] = 0;
-        fp[j] = fq[j] = 0;
+        const int i = base + j * PART_THREADS;
+        eo[j] = es[j] = 0;
+        int fp = 0, fq = 0;
         if (i < A.k) {
             node_of(i, A.level, A.k, eo[j], es[j]);
-            ep_[j] = A.P[i];
-            eq_[j] = A.Q[i];
             const int h = es[j] >> 1;
-            fp[j] = ep_[j] < h;
-            fq[j] = eq_[j] < h;
+            fp = A.P[i] < h;
+            fq = A.Q[i] < h;
         }
-        cp += fp[j];
-        cq += fq[j];
-    }
-    int xp = cp, xq = cq;
-    for (int off = 1; off < 32; off <<= 1) {
-        const int yp = __shfl_up_sync(FULL_MASK, xp, off), yq = __shfl_up_sync(FULL_MASK, xq, off);
-        if ((threadIdx.x & 31) >= off) {
-            xp += yp;
-            xq += yq;
+        const unsigned mp = __ballot_sync(FULL_MASK, fp), mq = __ballot_sync(FULL_MASK, fq);
+        if (lane == 0) {
+            gp[j * WARPS + w] = __popc(mp);
+            gq[j * WARPS + w] = __popc(mq);
         }
-    }
-    if ((threadIdx.x & 31) == 31) {
-        wp[threadIdx.x >> 5] = xp;
-        wq[threadIdx.x >> 5] = xq;
+        fbits |= unsigned(fp) << j;
+        gbits |= unsigned(fq) << j;
     }
     __syncthreads();
-    // Warp 0 publishes the tile's counts and looks back over its
-    // predecessors 32 at a time: lane l reads tile (front - 1 - l); the
-    // window's nearest INCL ends the look-back, otherwise its 32 AGG counts
-    // are added and the window moves back.  A window with a tile that has
-    // not published yet is read again (bounded by %globaltimer).
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        int tp = 0, tq = 0;
-        for (int w = 0; w < 8; ++w) {
-            tp += wp[w];
-            tq += wq[w];
+    // Warp 0 scans the group counts (lane l: groups GPL l .. GPL l + GPL - 1),
+    // publishes the tile's counts and looks back over its predecessors 32 at
+    // a time: lane l reads tile (front - 1 - l); the window's nearest INCL
+    // ends the look-back, otherwise its 32 AGG counts are added and the
+    // window moves back.  A window with a tile that has not published yet is
+    // read again (bounded by %globaltimer).
+    if (w == 0) {
+        int cp[GPL], cq[GPL], sp = 0, sq = 0;
+#pragma unroll
+        for (int t = 0; t < GPL; ++t) {
+            cp[t] = gp[GPL * lane + t];
+            cq[t] = gq[GPL * lane + t];
+            sp += cp[t];
+            sq += cq[t];
+        }
+        int xp = sp, xq = sq;
+        for (int off = 1; off < 32; off <<= 1) {
+            const int yp = __shfl_up_sync(FULL_MASK, xp, off), yq = __shfl_up_sync(FULL_MASK, xq, off);
+            if (lane >= off) {
+                xp += yp;
+                xq += yq;
+            }
+        }
+        const int tp = __shfl_sync(FULL_MASK, xp, 31), tq = __shfl_sync(FULL_MASK, xq, 31);
+        int rp = xp - sp, rq = xq - sq;
+#pragma unroll
+        for (int t = 0; t < GPL; ++t) {
+            gp[GPL * lane + t] = rp;
+            gq[GPL * lane + t] = rq;
+            rp += cp[t];
+            rq += cq[t];
         }
         int ep = 0, eq = 0;
         bool ok = true;
@@ -312,56 +338,47 @@ __global__ void __launch_bounds__(256) part_fused_kernel(FusedArgs F)
     }
     __syncthreads();
     if (!s_ok) return;
-    int op = s_ep, oq = s_eq;
-    for (int w = 0; w < (threadIdx.x >> 5); ++w) {
-        op += wp[w];
-        oq += wq[w];
-    }
-    op += xp - cp;
-    oq += xq - cq;
-    int sp[PER], sq[PER];
+    // The exclusive scan value of an entry over the whole level; only a
+    // node's first entry stores it (the scatter needs node-relative counts).
+    const int ep0 = s_ep, eq0 = s_eq;
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-        const int i = base + j;
-        sp[j] = op;
-        sq[j] = oq;
-        if (i < A.k) {
-            A.scanP[i] = op;
-            A.scanQ[i] = oq;
+        const int i = base + j * PART_THREADS;
+        const unsigned mp = __ballot_sync(FULL_MASK, (fbits >> j) & 1u);
+        const unsigned mq = __ballot_sync(FULL_MASK, (gbits >> j) & 1u);
+        if (i < A.k && i == eo[j]) {
+            A.scanP[i] = ep0 + gp[j * WARPS + w] + __popc(mp & below);
+            A.scanQ[i] = eq0 + gq[j * WARPS + w] + __popc(mq & below);
         }
-        op += fp[j];
-        oq += fq[j];
     }
     __threadfence();
     __syncthreads();
-    // This tile's scan values are written; then make sure those of the tile
-    // holding the node start of the tile's first entry are too.
+    // Node starts inside the tile are written; the one node that can start in
+    // an earlier tile is the node of the tile's first entry: wait for that
+    // tile's `done`.
     if (threadIdx.x == 0) {
         st_release_gpu(F.done + tile, 1);
         int o, sz;
-        node_of(tile * SCAN_BS, A.level, A.k, o, sz);
-        const int t_o = o / SCAN_BS;
+        node_of(tile * PART_BS, A.level, A.k, o, sz);
+        const int t_o = o / PART_BS;
         if (t_o < tile && !wait_done(F, t_o)) s_ok = 0;
     }
     __syncthreads();
     if (!s_ok) return;
     // Scan values at the node starts: written before the barrier above (this
     // tile) or before a done flag thread 0 acquired (an earlier tile); read
-    // through L2, the point of coherence, in one batch.
-    int so_p[PER], so_q[PER];
+    // through L2, the point of coherence.
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-        so_p[j] = base + j < A.k ? __ldcg(A.scanP + eo[j]) : 0;
-        so_q[j] = base + j < A.k ? __ldcg(A.scanQ + eo[j]) : 0;
-    }
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        const int i = base + j;
-        if (i >= A.k) break;
+        const int i = base + j * PART_THREADS;
+        const unsigned mp = __ballot_sync(FULL_MASK, (fbits >> j) & 1u);
+        const unsigned mq = __ballot_sync(FULL_MASK, (gbits >> j) & 1u);
+        if (i >= A.k) continue;
         const int o = eo[j], sz = es[j];
         const int h = sz >> 1;
-        const int p = ep_[j], q = eq_[j];
-        const int bp = sp[j] - so_p[j], bq = sq[j] - so_q[j];
+        const int p = A.P[i], q = A.Q[i];
+        const int bp = ep0 + gp[j * WARPS + w] + __popc(mp & below) - __ldcg(A.scanP + o);
+        const int bq = eq0 + gq[j * WARPS + w] + __popc(mq & below) - __ldcg(A.scanQ + o);
         const int local = i - o;
         const int pp = p < h ? o + bp : o + h + (local - bp);
         const int pq = q < h ? o + bq : o + h + (local - bq);
@@ -466,6 +483,62 @@ __device__ __forceinline__ void ant_walk(int dr, int dc, int delta, int s, int l
     }
 }
 
+// The same walk by a whole warp, as alternating runs: an up run climbs while
+// the row above adds nothing (delta stays 0), a right run moves while the
+// column adds nothing (delta stays -1), and the move that adds one ends the
+// run and turns the walk.  A fresh point can only lie where an up run starts:
+// every later position of the run was reached by a move whose row word added
+// nothing, and the test needs that word to add one.  Each run is found 32
+// moves at a time, lane l testing the word of the run's (t + 1 + l)-th move;
+// the first lane whose move turns the walk (or leaves the box) ends it.  (A
+// lone thread walking runs with branches was slower than the two-state step
+// above: lanes walking different nodes diverge.)  Lanes may read up
+// to 31 words past the walk's last move; rw / cw must accept any index
+// there (the window readers clamp), and their answers are not used.  Every
+// lane returns with the same state; lane 0 writes the fresh points.
+template <typename RowW, typename ColW, typename Put>
+__device__ __forceinline__ void ant_walk_warp(int dr, int dc, int delta, int s, int last, RowW rw, ColW cw, Put put,
+                                              int lane)
+{
+    if (delta != 0 && delta != -1) {
+        if (lane == 0) ant_walk_general(dr, dc, delta, s, last, rw, cw, put);
+        return;
+    }
+    if (!(dr >= 0 && dc <= s && dc - dr <= last)) return;
+    int left = int(min(int64_t(last) - (dc - dr), int64_t(dr) + s - dc)) + 1;
+    bool up = delta == 0;
+    while (left > 0) {
+        int t = 0;
+        unsigned hit = 0;
+        if (up) {
+            if (lane == 0 && dc > 0 && word_inc(cw(dc - 1), dr) && word_inc(rw(dr), dc)) put(dr, dc - 1);
+            while (t < left) {
+                const int r = dr - (t + 1 + lane);
+                hit = __ballot_sync(FULL_MASK, r < 0 || word_inc(rw(r), dc) != 0);
+                if (hit) break;
+                t += 32;
+            }
+            if (!hit) return;
+            t += __ffs(hit);
+            if (t > left || dr - t < 0) return; // out of steps, or it left the box upwards
+            dr -= t;
+        } else {
+            while (t < left) {
+                const int c = dc + t + lane;
+                hit = __ballot_sync(FULL_MASK, c >= s || word_inc(cw(c), dr) != 0);
+                if (hit) break;
+                t += 32;
+            }
+            if (!hit) return;
+            t += __ffs(hit);
+            if (t > left || dc + t > s) return; // out of steps, or it left the box to the right
+            dc += t;
+        }
+        left -= t;
+        up = !up;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // block-wide scans for the subtree kernel
 // ---------------------------------------------------------------------------
@@ -517,12 +590,55 @@ struct SubArgs {
     const int32_t *bad;
 };
 
+// Nodes below a subtree block's node (size S): the halving tree of S.  When S
+// is a power of two every node of depth d has size S >> d and starts at a
+// multiple of it, so the lookups are bit operations; otherwise node_of walks
+// down from the top.
+struct SubNodes {
+    int S;
+    bool pow2;
+    __device__ __forceinline__ void at(int i, int d, int &o, int &s) const
+    {
+        if (pow2) {
+            s = S >> d;
+            o = i & ~(s - 1);
+        } else {
+            node_of(i, d, S, o, s);
+        }
+    }
+    // node nd (0-based, left to right) of depth d
+    __device__ __forceinline__ void nth(int nd, int d, int &o, int &s) const
+    {
+        if (pow2) {
+            s = S >> d;
+            o = nd * s;
+            return;
+        }
+        o = 0;
+        s = S;
+        for (int e = 0; e < d; ++e) {
+            const int h = s >> 1;
+            if ((nd >> (d - 1 - e)) & 1) {
+                o += h;
+                s -= h;
+            } else {
+                s = h;
+            }
+        }
+    }
+};
+
 // One block finishes the subtree of one node of level lc (size <= MAXN):
-// every deeper level, down then up, in shared memory.  Smaller variants
+// every deeper level, down then up, in shared memory (the per-level maps,
+// child index -> parent-local index, in global memory).  Smaller variants
 // (fewer threads, less shared memory) keep more blocks resident per SM when
 // the cutoff is small.
+// Blocks kept resident per SM (bounds the registers): 12, 5 and 2 for the
+// 128-, 256- and 512-thread variants.
+constexpr int subtree_min_blocks(int threads) { return threads <= 128 ? 12 : (threads <= 256 ? 5 : 2); }
+
 template <int MAXN, int THREADS>
-__global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
+__global__ void __launch_bounds__(THREADS, subtree_min_blocks(THREADS)) subtree_kernel(SubArgs A)
 {
     if (*A.bad) return;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -537,6 +653,7 @@ __global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
             S = h;
         }
     }
+    const SubNodes N{S, S > 0 && (S & (S - 1)) == 0};
     int32_t *CW = reinterpret_cast<int32_t *>(smem); // row words of the node being walked
     int32_t *RW = CW + MAXN;                         // column words
     int16_t *Pa = reinterpret_cast<int16_t *>(RW + MAXN);
@@ -546,6 +663,9 @@ __global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
     int16_t *ResA = Qb + MAXN;
     int16_t *ResB = ResA + MAXN;
     __shared__ int wa[32], wb[32];
+    // map words of depth d below this block's node (child index -> parent-local index)
+    int32_t *maps0 = A.maps + size_t(2) * A.k * (A.lc + 1) + o;
+    auto pmap_of = [&](int d) { return maps0 + size_t(2) * A.k * d; };
 
     for (int i = threadIdx.x; i < S; i += THREADS) {
         Pa[i] = int16_t(A.P[o + i]);
@@ -567,7 +687,7 @@ __global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
             fp[j] = fq[j] = 0;
             if (i < S) {
                 int so, ss;
-                node_of(i, d, S, so, ss);
+                N.at(i, d, so, ss);
                 const int h = ss >> 1;
                 fp[j] = Pa[i] < h;
                 fq[j] = Qa[i] < h;
@@ -589,27 +709,25 @@ __global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
             eq += fq[j];
         }
         __syncthreads();
-        int32_t *pmap = A.maps + size_t(2) * A.k * (A.lc + d + 1);
-        int32_t *qmap = pmap + A.k;
         for (int i = threadIdx.x; i < S; i += THREADS) {
             int so, ss;
-            node_of(i, d, S, so, ss);
+            N.at(i, d, so, ss);
             const int h = ss >> 1, local = i - so;
             const int p = Pa[i], q = Qa[i];
             if (ss <= 1) {
                 Pb[i] = int16_t(p);
                 Qb[i] = int16_t(q);
-                pmap[o + i] = 0;
-                qmap[o + i] = 0;
+                pmap_of(d)[i] = 0;
+                pmap_of(d)[A.k + i] = 0;
                 continue;
             }
             const int bp = ResA[i] - ResA[so], bq = ResB[i] - ResB[so];
             const int pp = p < h ? so + bp : so + h + (local - bp);
             const int pq = q < h ? so + bq : so + h + (local - bq);
             Pb[pp] = int16_t(p < h ? p : p - h);
-            pmap[o + pp] = local;
             Qb[pq] = int16_t(q < h ? q : q - h);
-            qmap[o + pq] = local;
+            pmap_of(d)[pp] = local;
+            pmap_of(d)[A.k + pq] = local;
         }
         __syncthreads();
         int16_t *t = Pa;
@@ -625,19 +743,17 @@ __global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
     __syncthreads();
 
     for (int d = depth - 1; d >= 0; --d) {
-        const int32_t *pmap = A.maps + size_t(2) * A.k * (A.lc + d + 1);
-        const int32_t *qmap = pmap + A.k;
         // glue: children at level d+1 into parents at level d
         for (int i = threadIdx.x; i < S; i += THREADS) {
             int po, ps, co, cs;
-            node_of(i, d, S, po, ps);
+            N.at(i, d, po, ps);
             if (ps <= 1) {
                 ResA[i] = 0;
                 continue;
             }
-            node_of(i, d + 1, S, co, cs);
-            const int prow = pmap[o + i];
-            const int pcol = qmap[o + co + ResB[i]];
+            N.at(i, d + 1, co, cs);
+            const int prow = pmap_of(d)[i];
+            const int pcol = pmap_of(d)[A.k + co + ResB[i]];
             const int hi = co != po ? INT_MIN : 0;
             CW[po + prow] = pcol | hi;
             RW[po + pcol] = prow | hi;
@@ -645,23 +761,16 @@ __global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
         __syncthreads();
         for (int i = threadIdx.x; i < S; i += THREADS) {
             int po, ps;
-            node_of(i, d, S, po, ps);
+            N.at(i, d, po, ps);
             if (ps > 1) ResA[i] = int16_t(CW[i] & INT_MAX);
         }
         __syncthreads();
-        // walks: one thread per node of level d
+        // walks: one thread per node of level d (threads of a warp walking
+        // different nodes side by side)
         const int nodes = 1 << d;
         for (int nd = threadIdx.x; nd < nodes; nd += THREADS) {
-            int po = 0, ps = S;
-            for (int e = 0; e < d; ++e) {
-                const int h = ps >> 1;
-                if ((nd >> (d - 1 - e)) & 1) {
-                    po += h;
-                    ps -= h;
-                } else {
-                    ps = h;
-                }
-            }
+            int po, ps;
+            N.nth(nd, d, po, ps);
             if (ps <= 1) continue;
             const int32_t *cw_ = CW + po, *rw_ = RW + po;
             int16_t *res_ = ResA + po;
@@ -674,6 +783,27 @@ __global__ void __launch_bounds__(THREADS) subtree_kernel(SubArgs A)
         ResB = t;
     }
     for (int i = threadIdx.x; i < S; i += THREADS) A.res[o + i] = S > 1 ? ResB[i] : 0;
+}
+
+// A subtree launch; variants above 48 KB of shared memory opt in once per device.
+template <int MAXN, int THREADS>
+slcs_status launch_subtree(const SubArgs &S, int blocks, cudaStream_t st)
+{
+    constexpr size_t smem = subtree_smem(MAXN);
+    if (smem > 48 * 1024) {
+        static bool attr[64] = {};
+        int dev = 0;
+        SLCS_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) dev = 0;
+        if (!attr[dev]) {
+            SLCS_CUDA(cudaFuncSetAttribute(subtree_kernel<MAXN, THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int(smem)));
+            attr[dev] = true;
+        }
+    }
+    subtree_kernel<MAXN, THREADS><<<blocks, THREADS, smem, st>>>(S);
+    SLCS_CUDA(cudaGetLastError());
+    return SLCS_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -696,18 +826,28 @@ struct GlueArgs {
 __global__ void __launch_bounds__(256) glue_kernel(GlueArgs A)
 {
     if (*A.bad) return;
+    const bool pow2 = (A.k & (A.k - 1)) == 0;
+    int lg = 0; // log2 k for a power of two
+    while (pow2 && (1 << lg) < A.k) ++lg;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.k; i += gridDim.x * blockDim.x) {
-        // parent node (offset, size, index) and child node of entry i
+        // parent node (offset, size, index) and child node of entry i: for a
+        // power-of-two k every node of a level has size k >> level
         int po = 0, ps = A.k, nd = 0;
-        for (int d = 0; d < A.level; ++d) {
-            const int h = ps >> 1;
-            nd <<= 1;
-            if (i < po + h) {
-                ps = h;
-            } else {
-                po += h;
-                ps -= h;
-                nd |= 1;
+        if (pow2) {
+            ps = A.k >> A.level;
+            nd = i >> (lg - A.level);
+            po = nd * ps;
+        } else {
+            for (int d = 0; d < A.level; ++d) {
+                const int h = ps >> 1;
+                nd <<= 1;
+                if (i < po + h) {
+                    ps = h;
+                } else {
+                    po += h;
+                    ps -= h;
+                    nd |= 1;
+                }
             }
         }
         const int co = i < po + (ps >> 1) ? po : po + (ps >> 1);
@@ -981,14 +1121,30 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
         if (rlo > rhi) return;
         const int jj = E / B;
         const int ilo = rlo / B, ihi = rhi / B;
-        // first grid point of diagonal E with delta >= 0
+        // First grid point of diagonal E with delta >= 0 (delta does not
+        // decrease along a diagonal): the warp probes 32 evenly spaced points
+        // of the range at once and keeps the stretch where the test turns.
         int lo_i = ilo, hi_i = ihi + 1;
         while (lo_i < hi_i) {
-            const int mid = (lo_i + hi_i) >> 1;
-            if (T[mid * A.stride + mid + jj] >= 0) hi_i = mid;
-            else lo_i = mid + 1;
+            const int step = (hi_i - lo_i + 31) >> 5;
+            const int pi = lo_i + lane * step;
+            const bool ge = pi < hi_i && T[pi * A.stride + pi + jj] >= 0;
+            const unsigned inside = __ballot_sync(FULL_MASK, pi < hi_i);
+            const unsigned hit = __ballot_sync(FULL_MASK, ge);
+            if (hit & 1u) {
+                hi_i = lo_i; // the first point already passes
+                break;
+            }
+            if (hit) {
+                const int f = __ffs(hit) - 1;
+                const int nlo = lo_i + (f - 1) * step + 1;
+                hi_i = lo_i + f * step;
+                lo_i = nlo;
+            } else {
+                lo_i = lo_i + (31 - __clz(inside)) * step + 1; // past the last probe inside the range
+            }
         }
-        const int istar = lo_i;
+        const int istar = hi_i;
         int rstar;
         if (istar == ilo) {
             rstar = rlo;
@@ -1027,9 +1183,8 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
     }
     (void)G;
     // The segment walks at most B + 1 steps, each one row up or one column
-    // right, and reads words up to two steps ahead: rows [dr - B - 6, dr] and
-    // columns [dc - 1, dc + B + 5] cover it.  The warp stages them (coalesced) so that
-    // lane 0 walks in shared memory.
+    // right: rows [dr - B - 6, dr] and columns [dc - 1, dc + B + 5] cover
+    // them.  The warp stages them (coalesced), then walks in shared memory.
     const int wi = threadIdx.x >> 5;
     const int win = walk_win(B);
     int32_t *wr_s = walk_smem + size_t(wi) * 2 * win, *wc_s = wr_s + win;
@@ -1040,21 +1195,21 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
 #pragma unroll 4
     for (int t = lane; t < nc; t += 32) wc_s[t] = __ldg(A.RW + o + cb + t);
     __syncwarp();
-    if (lane != 0) return;
     const int32_t *wr = wr_s, *wc = wc_s;
     if (B + 12 <= WALK_WIN) {
-        // The window holds every row and column the walk reads (see above):
-        // shared memory only.  The index is clamped to the window, which
-        // changes nothing for the reads the walk makes and keeps any other
-        // inside the warp's own slice.
+        // The window holds every row and column the walk's moves read (see
+        // above): shared memory only.  The index is clamped to the window,
+        // which changes nothing for those reads and keeps the lanes' reads
+        // past the walk's end inside the warp's own slice.
         const unsigned rmax = unsigned(win - 1);
-        ant_walk(
+        ant_walk_warp(
             dr, dc, delta, s, E + B, [&](int r) { return wr[min(unsigned(r - rb), rmax)]; },
-            [&](int c) { return wc[min(unsigned(c - cb), rmax)]; }, [&](int r, int c) { A.res[o + r] = c; });
+            [&](int c) { return wc[min(unsigned(c - cb), rmax)]; }, [&](int r, int c) { A.res[o + r] = c; }, lane);
         return;
     }
-    // Grids coarser than the window (k beyond 2^20): outside it, global memory.
-    ant_walk(
+    // Grids coarser than the window (k beyond 2^20): outside it, global
+    // memory (the walk reads rows in [0, dr] and columns in [dc - 1, s) only).
+    ant_walk_warp(
         dr, dc, delta, s, E + B,
         [&](int r) {
             const unsigned t = unsigned(r - rb);
@@ -1064,7 +1219,7 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
             const unsigned t = unsigned(c - cb);
             return t < unsigned(nc) ? wc[t] : __ldg(A.RW + o + c);
         },
-        [&](int r, int c) { A.res[o + r] = c; });
+        [&](int r, int c) { A.res[o + r] = c; }, lane);
 }
 
 // Levels with short segments (B <= WALK_LANE_B) have many segments: one
@@ -1376,7 +1531,7 @@ slcs_status braid_workspace_bytes(int p, int q, int k, int cutoff, size_t *bytes
     b += size_t(p) * sizeof(int32_t) + size_t(q) * sizeof(int32_t); // inverses
     b += 2 * kk * sizeof(int32_t);                         // map_row, map_col
     b += 64 * 256 + 256;                                    // alignment slack, flag
-    b += size_t(levels + 1) * ((size_t(std::max(k, 1)) + SCAN_BS - 1) / SCAN_BS) * 12 + 512; // partition tiles
+    b += size_t(levels + 1) * ((size_t(std::max(k, 1)) + 256 * PART_PER - 1) / (256 * PART_PER)) * 12 + 512; // partition tiles
     *bytes = b;
     return SLCS_OK;
 }
@@ -1426,7 +1581,8 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     // level), their done flags and tickets (one per level): zeroed by one
     // memset.
     const int lc = cutoff_level(k, cutoff); // first level whose nodes fit a block
-    const int kb = int((kk + SCAN_BS - 1) / SCAN_BS);
+    const int part_bs = part_threads(k) * PART_PER;
+    const int kb = int((kk + part_bs - 1) / part_bs);
     const size_t tile_words = size_t(lc) * size_t(kb);
     const size_t sync_bytes = 256 + tile_words * 8 + tile_words * 4 + 256;
     char *sync_area = take(sync_bytes);
@@ -1459,7 +1615,8 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
                     scanP, scanQ, bsP, bsQ, k, l, bad};
         FusedArgs F{A, tiles + size_t(l) * size_t(kb), done + size_t(l) * size_t(kb), tickets + l, bad,
                     device_status_word()};
-        part_fused_kernel<<<kb, 256, 0, st>>>(F);
+        if (part_threads(k) == 1024) part_fused_kernel<1024><<<kb, 1024, 0, st>>>(F);
+        else part_fused_kernel<256><<<kb, 256, 0, st>>>(F);
         std::swap(Pcur, Pnext);
         std::swap(Qcur, Qnext);
     }
@@ -1468,23 +1625,11 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         int smax = k; // largest node of level lc (floor/ceil halving)
         for (int l = 0; l < lc; ++l) smax = smax - (smax >> 1);
         SubArgs S{Pcur, Qcur, res + kk * size_t(lc), maps, k, lc, bad};
-        if (smax <= 256) {
-            subtree_kernel<256, 128><<<1 << lc, 128, subtree_smem(256), st>>>(S);
-        } else if (smax <= 1024) {
-            subtree_kernel<1024, 256><<<1 << lc, 256, subtree_smem(1024), st>>>(S);
-        } else {
-            static bool attr[64] = {};
-            int dev = 0;
-            cudaGetDevice(&dev);
-            if (dev < 0 || dev >= 64) dev = 0;
-            if (!attr[dev]) {
-                SLCS_CUDA(cudaFuncSetAttribute(subtree_kernel<SUB_MAX, SUB_THREADS>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, int(subtree_smem(SUB_MAX))));
-                attr[dev] = true;
-            }
-            subtree_kernel<SUB_MAX, SUB_THREADS><<<1 << lc, SUB_THREADS, subtree_smem(SUB_MAX), st>>>(S);
-        }
-        SLCS_CUDA(cudaGetLastError());
+        slcs_status ss;
+        if (smax <= 256) ss = launch_subtree<256, 128>(S, 1 << lc, st);
+        else if (smax <= 1024) ss = launch_subtree<1024, 256>(S, 1 << lc, st);
+        else ss = launch_subtree<SUB_MAX, SUB_THREADS>(S, 1 << lc, st);
+        if (ss != SLCS_OK) return ss;
     }
     // Levels above: glue, union, walk.
     for (int l = lc - 1; l >= 0; --l) {
