@@ -405,13 +405,6 @@ struct slcs_batch_plan {
     };
     std::vector<Chunk> chunks;
     cudaEvent_t chunk_start = nullptr;
-    // The chunked host run captured as one graph (pinned host buffers only),
-    // for the host pointers and strand width it was captured with: one launch
-    // per run instead of eight API calls per chunk, which the host could not
-    // issue as fast as the chunks comb.
-    cudaGraphExec_t hgexec = nullptr;
-    const void *hg_a = nullptr, *hg_b = nullptr, *hg_out = nullptr;
-    int hg_bits = 0;
 
     CombLaunch launch(const uint8_t *a, const uint8_t *b, int32_t *out) const
     {
@@ -1175,104 +1168,6 @@ slcs_status slcs_batch_plan_run(slcs_batch_plan *P, const uint8_t *a, const uint
     return SLCS_OK;
 }
 
-static void drop_host_graph(slcs_batch_plan *P)
-{
-    if (P->hgexec) cudaGraphExecDestroy(P->hgexec);
-    P->hgexec = nullptr;
-    P->hg_a = P->hg_b = P->hg_out = nullptr;
-}
-
-// Whether p is page-locked host memory (copies from it can be captured and
-// overlap the combing).
-static bool host_pinned(const void *p)
-{
-    if (!p) return false;
-    cudaPointerAttributes at{};
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return at.type == cudaMemoryTypeHost;
-}
-
-static slcs_status narrow16(const int32_t *in, int16_t *out, int64_t lo, int64_t hi, cudaStream_t st);
-
-// The chunks of a host run, each on its own stream forked from and joined
-// back to `origin`: copy its ranges in, comb, (narrow,) copy its strands out.
-// direct: each chunk through slcs_batch_plan_run (its own graph); otherwise
-// the chunk's launch is enqueued as is (for a capture).
-static slcs_status enqueue_host_chunks(slcs_batch_plan *P, cudaStream_t origin, const uint8_t *a, const uint8_t *b,
-                                       void *out, int bits, uint8_t *da, uint8_t *db, int32_t *dout, int16_t *d16,
-                                       bool direct)
-{
-    SLCS_CUDA(cudaEventRecord(P->chunk_start, origin));
-    for (auto &k : P->chunks) {
-        SLCS_CUDA(cudaStreamWaitEvent(k.stream, P->chunk_start, 0));
-        if (k.a_hi > k.a_lo)
-            SLCS_CUDA(cudaMemcpyAsync(da + k.a_lo, a + k.a_lo, size_t(k.a_hi - k.a_lo), cudaMemcpyHostToDevice,
-                                      k.stream));
-        if (k.b_hi > k.b_lo)
-            SLCS_CUDA(cudaMemcpyAsync(db + k.b_lo, b + k.b_lo, size_t(k.b_hi - k.b_lo), cudaMemcpyHostToDevice,
-                                      k.stream));
-        slcs_status s = direct ? slcs_batch_plan_run(k.plan, da, db, dout, k.stream) : k.plan->enqueue(da, db, dout, k.stream);
-        if (s == SLCS_OK && bits == 16) s = narrow16(dout, d16, k.o_lo, k.o_hi, k.stream);
-        if (s != SLCS_OK) return s;
-        if (k.o_hi > k.o_lo) {
-            if (bits == 16)
-                SLCS_CUDA(cudaMemcpyAsync(static_cast<int16_t *>(out) + k.o_lo, d16 + k.o_lo,
-                                          sizeof(int16_t) * size_t(k.o_hi - k.o_lo), cudaMemcpyDeviceToHost, k.stream));
-            else
-                SLCS_CUDA(cudaMemcpyAsync(static_cast<int32_t *>(out) + k.o_lo, dout + k.o_lo,
-                                          sizeof(int32_t) * size_t(k.o_hi - k.o_lo), cudaMemcpyDeviceToHost, k.stream));
-        }
-        SLCS_CUDA(cudaEventRecord(k.done, k.stream));
-        SLCS_CUDA(cudaStreamWaitEvent(origin, k.done, 0));
-    }
-    return SLCS_OK;
-}
-
-// A chunked host run on stream st: as one graph when every host buffer is
-// pinned (captured on the first run with these pointers), else call by call.
-static slcs_status run_host_chunks(slcs_batch_plan *P, cudaStream_t st, const uint8_t *a, const uint8_t *b, void *out,
-                                   int bits, uint8_t *da, uint8_t *db, int32_t *dout, int16_t *d16)
-{
-    const bool graph = host_pinned(a) && host_pinned(b) && host_pinned(out);
-    if (!graph) {
-        slcs_status s = enqueue_host_chunks(P, st, a, b, out, bits, da, db, dout, d16, true);
-        if (s != SLCS_OK) return s;
-    } else {
-        if (!P->hgexec || P->hg_a != a || P->hg_b != b || P->hg_out != out || P->hg_bits != bits) {
-            if (P->hgexec) {
-                cudaGraphExecDestroy(P->hgexec);
-                P->hgexec = nullptr;
-            }
-            if (!P->cap_stream) SLCS_CUDA(cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking));
-            SLCS_CUDA(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal));
-            slcs_status s = enqueue_host_chunks(P, P->cap_stream, a, b, out, bits, da, db, dout, d16, false);
-            cudaGraph_t g = nullptr;
-            const cudaError_t e = cudaStreamEndCapture(P->cap_stream, &g);
-            if (s != SLCS_OK) {
-                if (g) cudaGraphDestroy(g);
-                return s;
-            }
-            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (host run)");
-            const cudaError_t ei = cudaGraphInstantiate(&P->hgexec, g, 0);
-            cudaGraphDestroy(g);
-            if (ei != cudaSuccess) {
-                P->hgexec = nullptr;
-                return cuda_fail(ei, "cudaGraphInstantiate (host run)");
-            }
-            P->hg_a = a;
-            P->hg_b = b;
-            P->hg_out = out;
-            P->hg_bits = bits;
-        }
-        SLCS_CUDA(cudaGraphLaunch(P->hgexec, st));
-    }
-    SLCS_CUDA(cudaStreamSynchronize(st));
-    return slcs_device_status(P->device, 1);
-}
-
 slcs_status slcs_batch_plan_run_host(slcs_batch_plan *P, const uint8_t *a, int64_t a_len, const uint8_t *b,
                                      int64_t b_len, int32_t *out, int64_t out_len, void *stream)
 {
@@ -1286,7 +1181,6 @@ slcs_status slcs_batch_plan_run_host(slcs_batch_plan *P, const uint8_t *a, int64
     const size_t need = ab + bb + sizeof(int32_t) * size_t(P->need_out) + 16;
     if (need > P->h_stage_bytes) {
         SLCS_CUDA(cudaStreamSynchronize(st));
-        drop_host_graph(P); // it holds the staging buffers' addresses
         cudaFree(P->h_stage);
         P->h_stage = nullptr;
         P->h_stage_bytes = 0;
@@ -1296,9 +1190,30 @@ slcs_status slcs_batch_plan_run_host(slcs_batch_plan *P, const uint8_t *a, int64
     uint8_t *da = reinterpret_cast<uint8_t *>(P->h_stage);
     uint8_t *db = reinterpret_cast<uint8_t *>(P->h_stage + ab);
     int32_t *dout = reinterpret_cast<int32_t *>(P->h_stage + ab + bb);
-    // Each chunk on its own stream: with pinned host buffers the copy
-    // engines move one chunk while another combs.
-    if (!P->chunks.empty()) return run_host_chunks(P, st, a, b, out, 32, da, db, dout, nullptr);
+    if (!P->chunks.empty()) {
+        // Each chunk on its own stream: copy its ranges in, comb, copy its
+        // strands out.  With pinned host buffers the copy engines move one
+        // chunk while another combs.
+        SLCS_CUDA(cudaEventRecord(P->chunk_start, st));
+        for (auto &k : P->chunks) {
+            SLCS_CUDA(cudaStreamWaitEvent(k.stream, P->chunk_start, 0));
+            if (k.a_hi > k.a_lo)
+                SLCS_CUDA(cudaMemcpyAsync(da + k.a_lo, a + k.a_lo, size_t(k.a_hi - k.a_lo), cudaMemcpyHostToDevice,
+                                          k.stream));
+            if (k.b_hi > k.b_lo)
+                SLCS_CUDA(cudaMemcpyAsync(db + k.b_lo, b + k.b_lo, size_t(k.b_hi - k.b_lo), cudaMemcpyHostToDevice,
+                                          k.stream));
+            slcs_status s = slcs_batch_plan_run(k.plan, da, db, dout, k.stream);
+            if (s != SLCS_OK) return s;
+            if (k.o_hi > k.o_lo)
+                SLCS_CUDA(cudaMemcpyAsync(out + k.o_lo, dout + k.o_lo, sizeof(int32_t) * size_t(k.o_hi - k.o_lo),
+                                          cudaMemcpyDeviceToHost, k.stream));
+            SLCS_CUDA(cudaEventRecord(k.done, k.stream));
+            SLCS_CUDA(cudaStreamWaitEvent(st, k.done, 0));
+        }
+        SLCS_CUDA(cudaStreamSynchronize(st));
+        return slcs_device_status(P->device, 1);
+    }
     if (P->need_a) SLCS_CUDA(cudaMemcpyAsync(da, a, size_t(P->need_a), cudaMemcpyHostToDevice, st));
     if (P->need_b) SLCS_CUDA(cudaMemcpyAsync(db, b, size_t(P->need_b), cudaMemcpyHostToDevice, st));
     slcs_status s = slcs_batch_plan_run(P, da, db, dout, stream);
@@ -1339,7 +1254,6 @@ slcs_status slcs_batch_plan_run_host16(slcs_batch_plan *P, const uint8_t *a, int
     const size_t need = ab + bb + sizeof(int32_t) * size_t(P->need_out) + 16;
     if (need > P->h_stage_bytes || size_t(P->need_out) > P->out16_elems) {
         SLCS_CUDA(cudaStreamSynchronize(st));
-        drop_host_graph(P); // it holds the staging buffers' addresses
         if (need > P->h_stage_bytes) {
             cudaFree(P->h_stage);
             P->h_stage = nullptr;
@@ -1359,10 +1273,31 @@ slcs_status slcs_batch_plan_run_host16(slcs_batch_plan *P, const uint8_t *a, int
     uint8_t *db = reinterpret_cast<uint8_t *>(P->h_stage + ab);
     int32_t *dout = reinterpret_cast<int32_t *>(P->h_stage + ab + bb);
     int16_t *d16 = P->d_out16;
-    // As slcs_batch_plan_run_host, chunk by chunk, with each chunk's strands
-    // narrowed on the device before they cross the bus (half the bytes of
-    // the copy back).
-    if (!P->chunks.empty()) return run_host_chunks(P, st, a, b, out, 16, da, db, dout, d16);
+    if (!P->chunks.empty()) {
+        // As slcs_batch_plan_run_host, chunk by chunk on their own streams,
+        // with each chunk's strands narrowed on the device before they cross
+        // the bus (half the bytes of the copy back).
+        SLCS_CUDA(cudaEventRecord(P->chunk_start, st));
+        for (auto &k : P->chunks) {
+            SLCS_CUDA(cudaStreamWaitEvent(k.stream, P->chunk_start, 0));
+            if (k.a_hi > k.a_lo)
+                SLCS_CUDA(cudaMemcpyAsync(da + k.a_lo, a + k.a_lo, size_t(k.a_hi - k.a_lo), cudaMemcpyHostToDevice,
+                                          k.stream));
+            if (k.b_hi > k.b_lo)
+                SLCS_CUDA(cudaMemcpyAsync(db + k.b_lo, b + k.b_lo, size_t(k.b_hi - k.b_lo), cudaMemcpyHostToDevice,
+                                          k.stream));
+            slcs_status s = slcs_batch_plan_run(k.plan, da, db, dout, k.stream);
+            if (s == SLCS_OK) s = narrow16(dout, d16, k.o_lo, k.o_hi, k.stream);
+            if (s != SLCS_OK) return s;
+            if (k.o_hi > k.o_lo)
+                SLCS_CUDA(cudaMemcpyAsync(out + k.o_lo, d16 + k.o_lo, sizeof(int16_t) * size_t(k.o_hi - k.o_lo),
+                                          cudaMemcpyDeviceToHost, k.stream));
+            SLCS_CUDA(cudaEventRecord(k.done, k.stream));
+            SLCS_CUDA(cudaStreamWaitEvent(st, k.done, 0));
+        }
+        SLCS_CUDA(cudaStreamSynchronize(st));
+        return slcs_device_status(P->device, 1);
+    }
     if (P->need_a) SLCS_CUDA(cudaMemcpyAsync(da, a, size_t(P->need_a), cudaMemcpyHostToDevice, st));
     if (P->need_b) SLCS_CUDA(cudaMemcpyAsync(db, b, size_t(P->need_b), cudaMemcpyHostToDevice, st));
     slcs_status s = slcs_batch_plan_run(P, da, db, dout, stream);
@@ -1384,7 +1319,6 @@ slcs_status slcs_batch_plan_destroy(slcs_batch_plan *P)
         if (k.done) cudaEventDestroy(k.done);
     }
     if (P->chunk_start) cudaEventDestroy(P->chunk_start);
-    if (P->hgexec) cudaGraphExecDestroy(P->hgexec);
     if (P->gexec) cudaGraphExecDestroy(P->gexec);
     if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
     cudaFree(P->d_pairs);
