@@ -1065,26 +1065,6 @@ __device__ __forceinline__ int colinc(const SegArgs &A, int o, int c, int r)
     return word_inc(__ldg(A.RW + o + c), r);
 }
 
-__device__ __forceinline__ int warp_sum(int v)
-{
-    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(FULL_MASK, v, off);
-    return v;
-}
-
-// Exact delta(r, c) (0 <= r, c <= s): table value at the grid point below-left
-// plus the steps down column c0 and along row r, summed by the warp.
-__device__ int delta_at(const SegArgs &A, const int32_t *T, int o, int r, int c, int lane)
-{
-    const int i0 = r / A.B, j0 = c / A.B;
-    const int r0 = i0 * A.B, c0 = j0 * A.B;
-    int acc = 0;
-#pragma unroll 4
-    for (int rr = r0 + lane; rr < r; rr += 32) acc += rowinc(A, o, rr, c0);
-#pragma unroll 4
-    for (int cc = c0 + lane; cc < c; cc += 32) acc += colinc(A, o, cc, r);
-    return T[i0 * A.stride + j0] + warp_sum(acc);
-}
-
 // Rows and columns a walk segment can touch, staged per warp in shared
 // memory (packed: position | hi flag in bit 31) before lane 0 walks.
 // Per warp two arrays of `win` words, win = min(B + 12, WALK_WIN) for the
@@ -1146,6 +1126,7 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
         }
         const int istar = hi_i;
         int rstar;
+        int dstart = T[ilo * A.stride + ilo + jj]; // delta(rlo, rlo + E): a grid point
         if (istar == ilo) {
             rstar = rlo;
         } else {
@@ -1171,6 +1152,7 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
                 const unsigned hit = __ballot_sync(FULL_MASK, r < rend && dval + pre >= 0);
                 if (hit) {
                     rstar = rb + __ffs(hit); // lane f (1-based) reaches row rb + f
+                    dstart = dval + __shfl_sync(FULL_MASK, pre, __ffs(hit) - 1);
                     break;
                 }
                 dval += __shfl_sync(FULL_MASK, pre, 31);
@@ -1178,8 +1160,9 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
         }
         dr = rstar - 1;
         dc = rstar + E;
-        if (dr < 0 || dc > s) return;
-        delta = delta_at(A, T, o, dr, dc, lane);
+        if (rstar > rhi || dr < 0 || dc > s) return;
+        // dstart = delta(r*, r* + E); one row up the point of row r* - 1 leaves
+        delta = dstart - rowinc(A, o, dr, dc);
     }
     (void)G;
     // The segment walks at most B + 1 steps, each one row up or one column
@@ -1227,18 +1210,6 @@ __global__ void __launch_bounds__(128) walk_segments_kernel(SegArgs A, int nodes
 // warp advances 32 walks at once instead of one.
 constexpr int WALK_LANE_B = 256;
 
-__device__ int delta_at_lane(const SegArgs &A, const int32_t *T, int o, int r, int c)
-{
-    const int i0 = r / A.B, j0 = c / A.B;
-    const int r0 = i0 * A.B, c0 = j0 * A.B;
-    int acc = T[i0 * A.stride + j0];
-#pragma unroll 4
-    for (int rr = r0; rr < r; ++rr) acc += rowinc(A, o, rr, c0);
-#pragma unroll 4
-    for (int cc = c0; cc < c; ++cc) acc += colinc(A, o, cc, r);
-    return acc;
-}
-
 __global__ void __launch_bounds__(256) walk_lanes_kernel(SegArgs A, int nodes)
 {
     if (*A.bad) return;
@@ -1271,8 +1242,9 @@ __global__ void __launch_bounds__(256) walk_lanes_kernel(SegArgs A, int nodes)
             else lo_i = mid + 1;
         }
         int rstar = rlo;
+        int dval = T[ilo * A.stride + ilo + jj]; // delta(rlo, rlo + E): a grid point
         if (lo_i != ilo) {
-            int dval = T[(lo_i - 1) * A.stride + (lo_i - 1) + jj];
+            dval = T[(lo_i - 1) * A.stride + (lo_i - 1) + jj];
             const int rend = min(lo_i * B, rhi);
             rstar = rhi + 1;
             for (int r = (lo_i - 1) * B; r < rend; ++r) {
@@ -1285,8 +1257,9 @@ __global__ void __launch_bounds__(256) walk_lanes_kernel(SegArgs A, int nodes)
         }
         dr = rstar - 1;
         dc = rstar + E;
-        if (dr < 0 || dc > s) return;
-        delta = delta_at_lane(A, T, o, dr, dc);
+        if (rstar > rhi || dr < 0 || dc > s) return;
+        // dval = delta(r*, r* + E); one row up the point of row r* - 1 leaves
+        delta = dval - rowinc(A, o, dr, dc);
     }
     ant_walk(
         dr, dc, delta, s, E + B, [&](int r) { return __ldg(A.CW + o + r); },
