@@ -1235,7 +1235,26 @@ __global__ void __launch_bounds__(256) walk_lanes_kernel(SegArgs A, int nodes)
         if (rlo > rhi) return;
         const int jj = E / B;
         const int ilo = rlo / B, ihi = rhi / B;
+        // first grid point of diagonal E with delta >= 0: three probes per
+        // round (read together), then halving
         int lo_i = ilo, hi_i = ihi + 1;
+        while (hi_i - lo_i > 3) {
+            const int w = hi_i - lo_i;
+            const int q1 = lo_i + w / 4, q2 = lo_i + w / 2, q3 = lo_i + 3 * w / 4;
+            const bool g1 = T[q1 * A.stride + q1 + jj] >= 0, g2 = T[q2 * A.stride + q2 + jj] >= 0,
+                       g3 = T[q3 * A.stride + q3 + jj] >= 0;
+            if (g1) {
+                hi_i = q1;
+            } else if (g2) {
+                lo_i = q1 + 1;
+                hi_i = q2;
+            } else if (g3) {
+                lo_i = q2 + 1;
+                hi_i = q3;
+            } else {
+                lo_i = q3 + 1;
+            }
+        }
         while (lo_i < hi_i) {
             const int mid = (lo_i + hi_i) >> 1;
             if (T[mid * A.stride + mid + jj] >= 0) hi_i = mid;
@@ -1247,11 +1266,19 @@ __global__ void __launch_bounds__(256) walk_lanes_kernel(SegArgs A, int nodes)
             dval = T[(lo_i - 1) * A.stride + (lo_i - 1) + jj];
             const int rend = min(lo_i * B, rhi);
             rstar = rhi + 1;
-            for (int r = (lo_i - 1) * B; r < rend; ++r) {
-                dval += colinc(A, o, r + E, r) + rowinc(A, o, r, r + E + 1);
-                if (dval >= 0) {
-                    rstar = r + 1;
-                    break;
+            // Four rows at a time: their words are read before any is tested,
+            // so that the reads' latency is paid once per four rows.
+            for (int r = (lo_i - 1) * B; r < rend && rstar > rhi; r += 4) {
+                int inc[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    inc[u] = r + u < rend ? colinc(A, o, r + u + E, r + u) + rowinc(A, o, r + u, r + u + E + 1) : 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (r + u < rend && rstar > rhi) {
+                        dval += inc[u];
+                        if (dval >= 0) rstar = r + u + 1;
+                    }
                 }
             }
         }
