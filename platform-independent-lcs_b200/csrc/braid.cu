@@ -908,7 +908,9 @@ __device__ __forceinline__ void node_by_index(int nd, int level, int k, int &o, 
 }
 
 // One warp per (node, row block): exclusive prefix of the hi counts and
-// inclusive suffix of the lo counts along the row, 32 columns per step.
+// inclusive suffix of the lo counts along the row, 32 columns per step, the
+// two scans side by side (hi from the left, lo from the right) with the next
+// step's words read before this step's scan.
 __global__ void __launch_bounds__(256) table_rows_kernel(TableArgs A, int nodes)
 {
     if (*A.bad) return;
@@ -922,56 +924,67 @@ __global__ void __launch_bounds__(256) table_rows_kernel(TableArgs A, int nodes)
     if (bi > G) return;
     int32_t *hi = A.cnt_hi + size_t(nd) * A.stride * A.stride + size_t(bi) * A.stride;
     int32_t *lo = A.cnt_lo + size_t(nd) * A.stride * A.stride + size_t(bi) * A.stride;
-    int carry = 0;
-    for (int base = 0; base <= G; base += 32) {
-        const int j = base + lane;
-        const int v = j <= G ? hi[j] : 0;
-        int x = v;
-        for (int off = 1; off < 32; off <<= 1) {
-            const int y = __shfl_up_sync(FULL_MASK, x, off);
-            if (lane >= off) x += y;
+    const int nch = G / 32 + 1; // steps of 32 columns over 0..G
+    int nh = lane <= G ? hi[lane] : 0;
+    int nl = (nch - 1) * 32 + lane <= G ? lo[(nch - 1) * 32 + lane] : 0;
+    int carry_h = 0, carry_l = 0;
+    for (int c = 0; c < nch; ++c) {
+        const int jh = c * 32 + lane, jl = (nch - 1 - c) * 32 + lane;
+        const int vh = nh, vl = nl;
+        if (c + 1 < nch) {
+            nh = jh + 32 <= G ? hi[jh + 32] : 0;
+            nl = lo[jl - 32]; // jl - 32 <= G - 32 + 31 < G
         }
-        if (j <= G) hi[j] = carry + x - v;
-        carry += __shfl_sync(FULL_MASK, x, 31);
-    }
-    carry = 0;
-    for (int base = (G / 32) * 32; base >= 0; base -= 32) {
-        const int j = base + lane;
-        int x = j <= G ? lo[j] : 0; // becomes the sum over lanes >= lane
+        int xh = vh, xl = vl; // xl becomes the sum over lanes >= lane
         for (int off = 1; off < 32; off <<= 1) {
-            const int y = __shfl_down_sync(FULL_MASK, x, off);
-            if (lane + off < 32) x += y;
+            const int yh = __shfl_up_sync(FULL_MASK, xh, off);
+            const int yl = __shfl_down_sync(FULL_MASK, xl, off);
+            if (lane >= off) xh += yh;
+            if (lane + off < 32) xl += yl;
         }
-        if (j <= G) lo[j] = carry + x;
-        carry += __shfl_sync(FULL_MASK, x, 0);
+        if (jh <= G) hi[jh] = carry_h + xh - vh;
+        if (jl <= G) lo[jl] = carry_l + xl;
+        carry_h += __shfl_sync(FULL_MASK, xh, 31);
+        carry_l += __shfl_sync(FULL_MASK, xl, 0);
     }
 }
 
-// One block per (node, 32 grid columns): a three-phase scan down the rows
-// (32 row chunks per column, coalesced across the columns) that finishes the
-// 2D sums and stores delta(iB, jB) = hi-prefix - lo-suffix in the hi table.
-__global__ void __launch_bounds__(1024) table_cols_kernel(TableArgs A, int nodes)
+// One block per (node, TCOL_COLS grid columns): a three-phase scan down the
+// rows (TCOL_CHUNKS row chunks per column; the chunk's words stay in
+// registers between the phases) that finishes the 2D sums and stores
+// delta(iB, jB) = hi-prefix - lo-suffix in the hi table.  Four columns per
+// block keep the top levels (one or two nodes of up to 1025 columns) on all
+// the SMs.
+constexpr int TCOL_COLS = 4;
+constexpr int TCOL_CHUNKS = 64;
+constexpr int TCOL_PER = (WALK_GMAX + 1 + TCOL_CHUNKS - 1) / TCOL_CHUNKS; // rows of a chunk, at most
+__global__ void __launch_bounds__(TCOL_COLS * TCOL_CHUNKS) table_cols_kernel(TableArgs A, int nodes)
 {
     if (*A.bad) return;
-    const int colblocks = (A.stride + 31) / 32;
+    const int colblocks = (A.stride + TCOL_COLS - 1) / TCOL_COLS;
     const int nd = blockIdx.x / colblocks, jb = blockIdx.x % colblocks;
     int o, s;
     node_by_index(nd, A.level, A.k, o, s);
     const int G = s / A.B;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int j = jb * 32 + tx;
+    const int tx = threadIdx.x % TCOL_COLS, ty = threadIdx.x / TCOL_COLS;
+    const int j = jb * TCOL_COLS + tx;
     const bool col_ok = j <= G;
-    const int rows = G + 1, per = (rows + 31) / 32;
+    const int rows = G + 1, per = (rows + TCOL_CHUNKS - 1) / TCOL_CHUNKS;
     const int i0 = min(rows, ty * per), i1 = min(rows, i0 + per);
     int32_t *hi = A.cnt_hi + size_t(nd) * A.stride * A.stride + j;
-    int32_t *lo = A.cnt_lo + size_t(nd) * A.stride * A.stride + j;
-    __shared__ int Hs[32][33], Ls[32][33];
+    const int32_t *lo = A.cnt_lo + size_t(nd) * A.stride * A.stride + j;
+    __shared__ int Hs[TCOL_CHUNKS][TCOL_COLS + 1], Ls[TCOL_CHUNKS][TCOL_COLS + 1];
+    int vh[TCOL_PER], vl[TCOL_PER];
     int hs = 0, ls = 0;
-    if (col_ok) {
-#pragma unroll 8
-        for (int i = i0; i < i1; ++i) {
-            hs += hi[size_t(i) * A.stride];
-            ls += lo[size_t(i) * A.stride];
+    {
+        const int32_t *ph = hi + size_t(i0) * A.stride, *pl = lo + size_t(i0) * A.stride;
+        const int n = col_ok ? i1 - i0 : 0;
+#pragma unroll
+        for (int u = 0; u < TCOL_PER; ++u) {
+            vh[u] = u < n ? ph[u * A.stride] : 0;
+            vl[u] = u < n ? pl[u * A.stride] : 0;
+            hs += vh[u];
+            ls += vl[u];
         }
     }
     Hs[ty][tx] = hs;
@@ -979,20 +992,16 @@ __global__ void __launch_bounds__(1024) table_cols_kernel(TableArgs A, int nodes
     __syncthreads();
     int hoff = 0, loff = 0;
     for (int t = 0; t < ty; ++t) hoff += Hs[t][tx];
-    for (int t = ty + 1; t < 32; ++t) loff += Ls[t][tx];
+    for (int t = ty + 1; t < TCOL_CHUNKS; ++t) loff += Ls[t][tx];
     if (!col_ok) return;
-    int run = loff;
-#pragma unroll 4
-    for (int i = i1 - 1; i >= i0; --i) {
-        run += lo[size_t(i) * A.stride];
-        lo[size_t(i) * A.stride] = run; // #lo points with row >= iB, col >= jB
-    }
-    run = hoff;
-#pragma unroll 4
-    for (int i = i0; i < i1; ++i) {
-        const int v = hi[size_t(i) * A.stride];
-        hi[size_t(i) * A.stride] = run - lo[size_t(i) * A.stride]; // delta(iB, jB)
-        run += v;
+    int run_h = hoff, run_l = loff + ls; // #lo points with row >= i0 + u, col >= jB
+    int32_t *ph = hi + size_t(i0) * A.stride;
+    const int n = i1 - i0;
+#pragma unroll
+    for (int u = 0; u < TCOL_PER; ++u) {
+        if (u < n) ph[u * A.stride] = run_h - run_l; // delta(iB, jB)
+        run_h += vh[u];
+        run_l -= vl[u];
     }
 }
 
@@ -1650,7 +1659,7 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         } else {
             const int rows = nodes * stride;
             table_rows_kernel<<<int((long(rows) * 32 + 255) / 256), 256, 0, st>>>(TA, nodes);
-            table_cols_kernel<<<nodes * ((stride + 31) / 32), 1024, 0, st>>>(TA, nodes);
+            table_cols_kernel<<<nodes * ((stride + TCOL_COLS - 1) / TCOL_COLS), TCOL_COLS * TCOL_CHUNKS, 0, st>>>(TA, nodes);
         }
         int smax = k;
         for (int d = 0; d < l; ++d) smax = smax - (smax >> 1);
