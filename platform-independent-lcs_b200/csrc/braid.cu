@@ -949,17 +949,19 @@ __global__ void __launch_bounds__(256) table_rows_kernel(TableArgs A, int nodes)
     }
 }
 
-// One block per (node, TCOL_COLS grid columns): a three-phase scan down the
-// rows (TCOL_CHUNKS row chunks per column; the chunk's words stay in
-// registers between the phases) that finishes the 2D sums and stores
-// delta(iB, jB) = hi-prefix - lo-suffix in the hi table.  Four columns per
-// block keep the top levels (one or two nodes of up to 1025 columns) on all
-// the SMs.
-constexpr int TCOL_COLS = 4;
-constexpr int TCOL_CHUNKS = 64;
-constexpr int TCOL_PER = (WALK_GMAX + 1 + TCOL_CHUNKS - 1) / TCOL_CHUNKS; // rows of a chunk, at most
-__global__ void __launch_bounds__(TCOL_COLS * TCOL_CHUNKS) table_cols_kernel(TableArgs A, int nodes)
+// One block per (node, COLS grid columns): a three-phase scan down the rows
+// (CHUNKS row chunks per column; the chunk's words stay in registers between
+// the phases) that finishes the 2D sums and stores delta(iB, jB) =
+// hi-prefix - lo-suffix in the hi table.  Large tables (the top levels: one
+// or two nodes of up to 1025 columns) take 4 columns x 64 row chunks per
+// block, so that they still spread over all the SMs; small ones (many nodes
+// of at most TCOL_SMALL_ROWS rows) 32 columns x 8 chunks.
+constexpr int TCOL_PER = (WALK_GMAX + 1 + 63) / 64; // rows of a chunk, at most
+constexpr int TCOL_SMALL_ROWS = 8 * TCOL_PER;
+template <int COLS, int CHUNKS>
+__global__ void __launch_bounds__(COLS * CHUNKS) table_cols_kernel(TableArgs A, int nodes)
 {
+    constexpr int TCOL_COLS = COLS, TCOL_CHUNKS = CHUNKS;
     if (*A.bad) return;
     const int colblocks = (A.stride + TCOL_COLS - 1) / TCOL_COLS;
     const int nd = blockIdx.x / colblocks, jb = blockIdx.x % colblocks;
@@ -1659,7 +1661,10 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         } else {
             const int rows = nodes * stride;
             table_rows_kernel<<<int((long(rows) * 32 + 255) / 256), 256, 0, st>>>(TA, nodes);
-            table_cols_kernel<<<nodes * ((stride + TCOL_COLS - 1) / TCOL_COLS), TCOL_COLS * TCOL_CHUNKS, 0, st>>>(TA, nodes);
+            if (stride <= TCOL_SMALL_ROWS)
+                table_cols_kernel<32, 8><<<nodes * ((stride + 31) / 32), 256, 0, st>>>(TA, nodes);
+            else
+                table_cols_kernel<4, 64><<<nodes * ((stride + 3) / 4), 256, 0, st>>>(TA, nodes);
         }
         int smax = k;
         for (int d = 0; d < l; ++d) smax = smax - (smax >> 1);
