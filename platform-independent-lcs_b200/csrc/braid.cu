@@ -633,6 +633,114 @@ struct SubNodes {
 // child index -> parent-local index, in global memory).  Smaller variants
 // (fewer threads, less shared memory) keep more blocks resident per SM when
 // the cutoff is small.
+// The walk of one node (offset po, size ps) inside a subtree block, cut into
+// segments like the walks of the levels above the cutoff: a delta table of
+// SUB_G + 1 grid lines per dimension (spacing B = ps / SUB_G, rounded up) is
+// counted and summed in shared memory, then thread q walks segment q: the
+// diagonals (E, E + B] with E = (q - ceil(ps / B)) B, from one row above
+// r*(E), the first row of diagonal E whose delta is >= 0 (a search of the
+// table along the diagonal, then a scan of at most B rows).  Every thread of
+// the block calls it (it synchronises the block).
+constexpr int SUB_G = 16;
+constexpr int SUB_TAB = (SUB_G + 1) * (SUB_G + 1);
+template <int THREADS>
+__device__ void sub_walk_segmented(const int32_t *CW, const int32_t *RW, int16_t *Res, int po, int ps, int32_t *Th,
+                                   int32_t *Tl)
+{
+    const int B = (ps + SUB_G - 1) / SUB_G;
+    const int G = ps / B, W = G + 1;
+    for (int i = threadIdx.x; i < W * W; i += THREADS) {
+        Th[i] = 0;
+        Tl[i] = 0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < ps; r += THREADS) {
+        const int w = CW[po + r];
+        const int bi = min(r / B, G), bj = min((w & INT_MAX) / B, G);
+        atomicAdd((w < 0 ? Th : Tl) + bi * W + bj, 1);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < W; i += THREADS) { // rows: hi exclusive prefix, lo inclusive suffix
+        int run = 0;
+        for (int j = 0; j < W; ++j) {
+            const int v = Th[i * W + j];
+            Th[i * W + j] = run;
+            run += v;
+        }
+        run = 0;
+        for (int j = G; j >= 0; --j) {
+            run += Tl[i * W + j];
+            Tl[i * W + j] = run;
+        }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < W; j += THREADS) { // columns, then delta into the hi table
+        int run = 0;
+        for (int i = G; i >= 0; --i) {
+            run += Tl[i * W + j];
+            Tl[i * W + j] = run;
+        }
+        run = 0;
+        for (int i = 0; i < W; ++i) {
+            const int v = Th[i * W + j];
+            Th[i * W + j] = run - Tl[i * W + j];
+            run += v;
+        }
+    }
+    __syncthreads();
+    const int32_t *cw_ = CW + po, *rw_ = RW + po;
+    const int jmin = -((ps + B - 1) / B);
+    const int nseg = 2 * ((ps + B - 1) / B) + 2;
+    const int e0 = -(ps - 1);
+    for (int q = threadIdx.x; q < nseg; q += THREADS) {
+        const int E = (jmin + q) * B;
+        if (E > ps || E + B < e0) continue;
+        int dr, dc, delta;
+        if (E < e0) {
+            dr = ps - 1;
+            dc = 0;
+            delta = cw_[ps - 1] < 0 ? 0 : -1;
+        } else {
+            const int rlo = max(0, -E), rhi = min(ps, ps - E);
+            if (rlo > rhi) continue;
+            const int jj = E / B;
+            const int ilo = rlo / B, ihi = rhi / B;
+            int lo_i = ilo, hi_i = ihi + 1;
+            while (lo_i < hi_i) {
+                const int mid = (lo_i + hi_i) >> 1;
+                if (Th[mid * W + mid + jj] >= 0) hi_i = mid;
+                else lo_i = mid + 1;
+            }
+            int rstar = rlo;
+            int dval = Th[ilo * W + ilo + jj]; // delta(rlo, rlo + E): a grid point
+            if (lo_i != ilo) {
+                dval = Th[(lo_i - 1) * W + (lo_i - 1) + jj];
+                const int rend = min(lo_i * B, rhi);
+                rstar = rhi + 1;
+                for (int r = (lo_i - 1) * B; r < rend; ++r) {
+                    dval += word_inc(rw_[r + E], r) + word_inc(cw_[r], r + E + 1);
+                    if (dval >= 0) {
+                        rstar = r + 1;
+                        break;
+                    }
+                }
+            }
+            dr = rstar - 1;
+            dc = rstar + E;
+            if (rstar > rhi || dr < 0 || dc > ps) continue;
+            delta = dval - word_inc(cw_[dr], dc);
+        }
+        ant_walk(dr, dc, delta, ps, E + B, [&](int r) { return cw_[r]; }, [&](int c) { return rw_[c]; },
+                 [&](int r, int c) { Res[po + r] = int16_t(c); });
+    }
+    __syncthreads();
+}
+
+// Segmented walks inside a subtree block: nodes of at least SUB_SEG_MIN
+// entries on levels of at most SUB_SEG_NODES nodes.
+constexpr int SUB_SEG_MIN = 64;
+constexpr int SUB_SEG_NODES = 4;
+
 // Blocks kept resident per SM (bounds the registers): 12, 5 and 2 for the
 // 128-, 256- and 512-thread variants.
 constexpr int subtree_min_blocks(int threads) { return threads <= 128 ? 12 : (threads <= 256 ? 5 : 2); }
@@ -663,6 +771,7 @@ __global__ void __launch_bounds__(THREADS, subtree_min_blocks(THREADS)) subtree_
     int16_t *ResA = Qb + MAXN;
     int16_t *ResB = ResA + MAXN;
     __shared__ int wa[32], wb[32];
+    __shared__ int32_t sTh[SUB_TAB], sTl[SUB_TAB]; // delta table of a segmented walk
     // map words of depth d below this block's node (child index -> parent-local index)
     int32_t *maps0 = A.maps + size_t(2) * A.k * (A.lc + 1) + o;
     auto pmap_of = [&](int d) { return maps0 + size_t(2) * A.k * d; };
@@ -765,17 +874,27 @@ __global__ void __launch_bounds__(THREADS, subtree_min_blocks(THREADS)) subtree_
             if (ps > 1) ResA[i] = int16_t(CW[i] & INT_MAX);
         }
         __syncthreads();
-        // walks: one thread per node of level d (threads of a warp walking
-        // different nodes side by side)
+        // walks: the first levels (nodes of at least SUB_SEG_MIN entries, at
+        // most SUB_SEG_NODES of them) one node after the other, each cut into
+        // segments walked side by side; below, one thread per node (threads
+        // of a warp walking different nodes side by side)
         const int nodes = 1 << d;
-        for (int nd = threadIdx.x; nd < nodes; nd += THREADS) {
-            int po, ps;
-            N.nth(nd, d, po, ps);
-            if (ps <= 1) continue;
-            const int32_t *cw_ = CW + po, *rw_ = RW + po;
-            int16_t *res_ = ResA + po;
-            ant_walk(ps - 1, 0, cw_[ps - 1] < 0 ? 0 : -1, ps, INT_MAX, [&](int r) { return cw_[r]; },
-                     [&](int c) { return rw_[c]; }, [&](int r, int c) { res_[r] = int16_t(c); });
+        if (nodes <= SUB_SEG_NODES && (S >> d) >= SUB_SEG_MIN) {
+            for (int nd = 0; nd < nodes; ++nd) {
+                int po, ps;
+                N.nth(nd, d, po, ps);
+                if (ps > 1) sub_walk_segmented<THREADS>(CW, RW, ResA, po, ps, sTh, sTl);
+            }
+        } else {
+            for (int nd = threadIdx.x; nd < nodes; nd += THREADS) {
+                int po, ps;
+                N.nth(nd, d, po, ps);
+                if (ps <= 1) continue;
+                const int32_t *cw_ = CW + po, *rw_ = RW + po;
+                int16_t *res_ = ResA + po;
+                ant_walk(ps - 1, 0, cw_[ps - 1] < 0 ? 0 : -1, ps, INT_MAX, [&](int r) { return cw_[r]; },
+                         [&](int c) { return rw_[c]; }, [&](int r, int c) { res_[r] = int16_t(c); });
+            }
         }
         __syncthreads();
         int16_t *t = ResA;
