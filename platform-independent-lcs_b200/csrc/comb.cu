@@ -47,8 +47,12 @@ namespace slcs {
 namespace {
 
 constexpr int TN = 4;      // columns per step of the stream kernels (one 16-byte v vector)
-constexpr int PREF = 4;    // blocks lane 0 prefetches ahead
-constexpr int RING = 8;    // shared-memory ring slots per warp (> PREF)
+// Blocks lane 0 of a stripe prefetches ahead: 2 for stripes of at most 14
+// rows per lane, 4 for 16 (on B200 the 4096 pair took 0.83 ms instead of
+// 0.87 with 2, the 2^20 pair 300 instead of 302 ms; the 131072 pair's 16-row
+// stripes took 12.0 instead of 11.3 ms).
+__host__ __device__ constexpr int pref_of(int tm) { return tm >= 16 ? 4 : 2; }
+constexpr int RING = 8;    // shared-memory ring slots per warp (> the prefetch)
 constexpr int PUBLISH_COLS = 32; // columns between progress releases
 
 struct StripeWait {
@@ -100,6 +104,7 @@ __device__ __forceinline__ void cell(int a_sym, int b_sym, int &h, int &v)
 template <int TM, int TW>
 struct Stripe {
     static constexpr int Q = TW / 4;                 // int4 per block
+    static constexpr int PREF = pref_of(TM);
     static constexpr int PUBLISH = PUBLISH_COLS / TW; // blocks between releases
 
     const uint8_t *__restrict__ b;
@@ -253,7 +258,7 @@ __device__ __forceinline__ void comb_stripe(const CombLaunch &L, const PairDev &
 
     if (!S.first && lane == 0) {
 #pragma unroll
-        for (int d = 0; d < PREF; ++d) {
+        for (int d = 0; d < Stripe<TM, TW>::PREF; ++d) {
             if (d < nb) {
                 S.W.until(d);
                 if (!S.W.dead) {
