@@ -924,16 +924,20 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
             const int32_t n = std::max(pairs[it.first].n, it.second >= 0 ? pairs[it.second].n : 0);
             return int64_t((n + cols - 1) / cols) + 2;
         };
-        std::vector<double> wsteps(nclass, 0.0);
+        // Per class: its steps in total, its longest item, and how many warps
+        // can have work at all.
+        std::vector<double> csteps(nclass, 0.0), clong(nclass, 0.0);
         std::vector<long> wmax(nclass, 0);
-        double total = 0.0;
         for (int c = 0; c < nclass; ++c) {
-            int64_t w = 0;
-            for (const auto &it : items[c]) w += cost(c, it);
+            int64_t w = 0, longest = 0;
+            for (const auto &it : items[c]) {
+                w += cost(c, it);
+                longest = std::max(longest, cost(c, it));
+            }
             const int spw = 32 / P->classes[c].seg;
-            wsteps[c] = double(w) / spw * class_step_time(P->classes[c], P->tns);
+            csteps[c] = double(w);
+            clong[c] = double(longest);
             wmax[c] = (long(items[c].size()) + spw - 1) / spw;
-            total += wsteps[c];
         }
         const long want_wf = (long(P->ntasks) + BATCH_WARPS - 1) / BATCH_WARPS;
         long want = std::max<long>(1, want_wf);
@@ -948,20 +952,39 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
         // the 20,000-read launch).
         const long reserve = std::min<long>(P->ntasks, long(grid) * BATCH_WARPS / 8);
         const long warps_total = long(grid) * BATCH_WARPS - reserve;
+        // Warps per class so that the classes end together.  A class of w
+        // warps ends about when each of its w * spw segments has combed its
+        // share of the class's steps and the last one its longest item, half
+        // of which is still to go on average: end(w) = t * (S / (w * spw) +
+        // L / 2), t the class's time per step.  Each warp goes to the class
+        // that would end last.  (Shares in proportion to S * t alone gave the
+        // 385-512-row class of the 20,000 reads 30 warps for 64 items of
+        // ~150 steps: it ended ~40 us after every other class.)
         std::vector<long> wc(nclass, 0);
         long used = 0;
+        auto class_end = [&](int c, long w) {
+            const int spw = 32 / P->classes[c].seg;
+            return class_step_time(P->classes[c], P->tns) * (csteps[c] / double(w * spw) + clong[c] / 2.0);
+        };
         for (int c = 0; c < nclass; ++c) {
             if (items[c].empty()) continue;
-            long w = total > 0 ? long(double(warps_total) * wsteps[c] / total) : 1;
-            w = std::max(1L, std::min(w, wmax[c]));
-            wc[c] = w;
-            used += w;
+            wc[c] = 1;
+            ++used;
         }
-        while (used > warps_total) { // trim the largest allocations
-            int big = int(std::max_element(wc.begin(), wc.end()) - wc.begin());
-            if (wc[big] <= 1) break;
-            --wc[big];
-            --used;
+        while (used < warps_total) {
+            int worst = -1;
+            double worst_end = -1.0;
+            for (int c = 0; c < nclass; ++c) {
+                if (wc[c] == 0 || wc[c] >= wmax[c]) continue;
+                const double e = class_end(c, wc[c]);
+                if (e > worst_end) {
+                    worst_end = e;
+                    worst = c;
+                }
+            }
+            if (worst < 0) break; // every class has a warp per item
+            ++wc[worst];
+            ++used;
         }
         if (std::count_if(wc.begin(), wc.end(), [](long w) { return w > 0; }) > MAX_CLASSES) {
             delete P;

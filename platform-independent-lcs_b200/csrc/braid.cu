@@ -177,9 +177,26 @@ struct FusedArgs {
     LevelArgs L;
     unsigned long long *tiles; // status word per tile of this level, zero at launch
     int32_t *done;             // per tile of this level: scan values written (1), zero at launch
-    int32_t *ticket;           // tile ticket of this level, zero at launch
     int32_t *err;              // the product's error flag
     uint32_t *status;          // device status word
+};
+
+// Every level above the cutoff in one launch: tickets run level by level
+// (ticket t is tile t % kb of level t / kb), and a tile of level l first
+// waits until all kb tiles of level l - 1 have scattered (level_done), so
+// that it reads finished arrays.  Every wait targets smaller tickets, which
+// running blocks hold, so each ends; each is also bounded by %globaltimer.
+struct PartAllArgs {
+    int32_t *PQ;               // four k-arrays: P and Q of even levels, then of odd levels
+    int32_t *maps;             // level l + 1's pmap at maps + 2k(l + 1), its qmap k further
+    int32_t *scanP, *scanQ;
+    int k, levels, kb;         // levels above the cutoff, tiles per level
+    unsigned long long *tiles; // levels * kb tile status words, zero at launch
+    int32_t *done;             // levels * kb scan-written flags, zero at launch
+    int32_t *ticket;           // zero at launch
+    int32_t *level_done;       // per level: tiles scattered, zero at launch
+    int32_t *err;
+    uint32_t *status;
 };
 
 // Thread 0: spin until done[t] is set, bounded; false on expiry.
@@ -202,7 +219,17 @@ __device__ __forceinline__ bool wait_done(const FusedArgs &F, int t)
 }
 
 template <int PART_THREADS>
-__global__ void __launch_bounds__(PART_THREADS) part_fused_kernel(FusedArgs F)
+struct PartSmem {
+    static constexpr int GROUPS = PART_PER * PART_THREADS / 32; // runs of 32 entries per tile
+    int s_ok;
+    int gp[GROUPS], gq[GROUPS]; // group counts, then their exclusive prefixes in the tile
+    int s_ep, s_eq;             // exclusive prefix of the tile
+};
+
+// One tile of one level: count, look back, scan, scatter.  False when the
+// product failed (err raised here or elsewhere); the block then stops.
+template <int PART_THREADS>
+__device__ __forceinline__ bool part_tile(const FusedArgs &F, int tile, PartSmem<PART_THREADS> &S)
 {
     const LevelArgs &A = F.L;
     constexpr int PER = PART_PER;
@@ -210,16 +237,9 @@ __global__ void __launch_bounds__(PART_THREADS) part_fused_kernel(FusedArgs F)
     constexpr int WARPS = PART_THREADS / 32;
     constexpr int GROUPS = PER * WARPS;         // runs of 32 entries per tile
     constexpr int GPL = GROUPS / 32;            // groups per lane of the scanning warp
-    __shared__ int s_tile, s_ok;
-    __shared__ int gp[GROUPS], gq[GROUPS]; // group counts, then their exclusive prefixes in the tile
-    __shared__ int s_ep, s_eq;             // exclusive prefix of the tile
-    if (threadIdx.x == 0) {
-        s_tile = atomicAdd(F.ticket, 1);
-        s_ok = !ld_relaxed_gpu(F.err);
-    }
-    __syncthreads();
-    if (!s_ok) return;
-    const int tile = s_tile;
+    int &s_ok = S.s_ok;
+    int *gp = S.gp, *gq = S.gq;
+    int &s_ep = S.s_ep, &s_eq = S.s_eq;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned below = (1u << lane) - 1u;
     // Striped: entry j of the thread is tile entry j * PART_THREADS +
@@ -337,7 +357,7 @@ __global__ void __launch_bounds__(PART_THREADS) part_fused_kernel(FusedArgs F)
         }
     }
     __syncthreads();
-    if (!s_ok) return;
+    if (!s_ok) return false;
     // The exclusive scan value of an entry over the whole level; only a
     // node's first entry stores it (the scatter needs node-relative counts).
     const int ep0 = s_ep, eq0 = s_eq;
@@ -364,7 +384,7 @@ __global__ void __launch_bounds__(PART_THREADS) part_fused_kernel(FusedArgs F)
         if (t_o < tile && !wait_done(F, t_o)) s_ok = 0;
     }
     __syncthreads();
-    if (!s_ok) return;
+    if (!s_ok) return false;
     // Scan values at the node starts: written before the barrier above (this
     // tile) or before a done flag thread 0 acquired (an earlier tile); read
     // through L2, the point of coherence.
@@ -394,7 +414,63 @@ __global__ void __launch_bounds__(PART_THREADS) part_fused_kernel(FusedArgs F)
         A.Qn[pq] = q < h ? q : q - h;
         A.qmap[pq] = local;
     }
+    return true;
 }
+
+template <int PART_THREADS>
+__global__ void __launch_bounds__(PART_THREADS) part_levels_kernel(PartAllArgs G)
+{
+    constexpr int PART_BS = PART_THREADS * PART_PER;
+    __shared__ PartSmem<PART_THREADS> S;
+    __shared__ int s_ticket;
+    const size_t kk = size_t(G.k);
+    for (;;) {
+        __syncthreads(); // the previous tile is done with the shared arrays
+        if (threadIdx.x == 0) {
+            s_ticket = atomicAdd(G.ticket, 1);
+            S.s_ok = !ld_relaxed_gpu(G.err);
+            const int lv = s_ticket / G.kb;
+            if (S.s_ok && lv > 0 && lv < G.levels) {
+                // every tile of the level above has scattered into this level's input
+                uint64_t t0 = 0;
+                while (ld_acquire_gpu(G.level_done + lv - 1) < G.kb) {
+                    if (ld_relaxed_gpu(G.err)) {
+                        S.s_ok = 0;
+                        break;
+                    }
+                    const uint64_t now = globaltimer_ns();
+                    if (t0 == 0) {
+                        t0 = now;
+                    } else if (now - t0 > PART_WAIT_NS) {
+                        atomicExch(G.err, 1);
+                        raise_status(G.status, DEV_ERR_TIMEOUT);
+                        S.s_ok = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        __syncthreads();
+        const int t = s_ticket;
+        if (!S.s_ok || t >= G.levels * G.kb) return;
+        const int lv = t / G.kb, tile = t % G.kb;
+        int32_t *in = G.PQ + ((lv & 1) ? 2 * kk : 0), *nx = G.PQ + ((lv & 1) ? 0 : 2 * kk);
+        int32_t *mp = G.maps + 2 * kk * size_t(lv + 1);
+        FusedArgs F{LevelArgs{in, in + kk, nx, nx + kk, mp, mp + kk, G.scanP, G.scanQ, nullptr, nullptr, G.k, lv,
+                              G.err},
+                    G.tiles + size_t(lv) * G.kb, G.done + size_t(lv) * G.kb, G.err, G.status};
+        if (!part_tile<PART_THREADS>(F, tile, S)) return;
+        (void)PART_BS;
+        __syncthreads(); // every thread of the tile has scattered
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(G.level_done + lv, 1);
+        }
+    }
+}
+
+
 
 // ---------------------------------------------------------------------------
 // the ant walk (ant_passage, src/braid_multiplication.hpp:123-189)
@@ -1426,21 +1502,20 @@ __global__ void __launch_bounds__(256) walk_lanes_kernel(SegArgs A, int nodes)
 // ---------------------------------------------------------------------------
 // staggered multiplication around the steady ant
 // ---------------------------------------------------------------------------
-// c2r = inverse of r2c; entries outside [0, n) raise *bad.  c2r must be -1 filled.
-__global__ void inverse_kernel(const int32_t *r2c, int32_t *c2r, int n, int32_t *bad)
+// Pc = inverse of P (p entries) and Qc = inverse of Q (q entries), one
+// launch; an entry outside [0, n) raises *bad.  A column that no entry hits
+// keeps whatever Pc / Qc held: slice_count_kernel detects it (a repeat in
+// the input leaves some column unhit).
+__global__ void inverse_pair_kernel(const int32_t *P, int32_t *Pc, int p, const int32_t *Q, int32_t *Qc, int q,
+                                    int32_t *bad)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int c = r2c[i];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < p + q; t += gridDim.x * blockDim.x) {
+        const bool in_p = t < p;
+        const int i = in_p ? t : t - p, n = in_p ? p : q;
+        const int c = in_p ? P[i] : Q[i];
         if (c < 0 || c >= n) *bad = 1;
-        else c2r[c] = i;
+        else (in_p ? Pc : Qc)[c] = i;
     }
-}
-
-// Every column must have been hit exactly once: a -1 left means a repeat.
-__global__ void check_full_kernel(const int32_t *c2r, int n, int32_t *bad)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        if (c2r[i] < 0) *bad = 1;
 }
 
 // Slices of P (rows whose column lies in [c0, c0+k), row order) and of Q
@@ -1449,13 +1524,14 @@ __global__ void check_full_kernel(const int32_t *c2r, int n, int32_t *bad)
 struct SliceArgs {
     const int32_t *P_r2c;
     const int32_t *Q_c2r;
+    const int32_t *P_c2r, *Q_r2c; // for the permutation check
     int p, q, k, c0, r0;
     int32_t *p_red;  // level-0 P (r2c, local)
     int32_t *q_red;  // level-0 Q (c2r, local)
     int32_t *map_row, *map_col;
     int32_t *scanP, *scanQ, *bsumP, *bsumQ;
     int n; // max(p, q)
-    const int32_t *bad;
+    int32_t *bad;
 };
 
 __device__ __forceinline__ void slice_flags(const SliceArgs &A, int i, int &fp, int &fq)
@@ -1470,6 +1546,16 @@ __global__ void __launch_bounds__(256) slice_count_kernel(SliceArgs A)
     const int base = blockIdx.x * SCAN_BS;
     int cp = 0, cq = 0;
     for (int i = base + threadIdx.x; i < min(base + SCAN_BS, A.n); i += blockDim.x) {
+        // Column i of P (row i of Q) must be the image of the row its
+        // inverse names: otherwise no entry hit it and the input repeats one.
+        if (i < A.p) {
+            const int r = A.P_c2r[i];
+            if (unsigned(r) >= unsigned(A.p) || A.P_r2c[r] != i) *A.bad = 1;
+        }
+        if (i < A.q) {
+            const int c = A.Q_c2r[i];
+            if (unsigned(c) >= unsigned(A.q) || A.Q_r2c[c] != i) *A.bad = 1;
+        }
         int fp, fq;
         slice_flags(A, i, fp, fq);
         cp += fp;
@@ -1555,11 +1641,15 @@ struct AssembleArgs {
     int p, q, k;
     bool row_glue;
     const int32_t *bad;
+    uint32_t *status;   // device status word: DEV_ERR_INPUT when the product failed
 };
 
 __global__ void __launch_bounds__(256) assemble_kernel(AssembleArgs A)
 {
-    if (*A.bad) return;
+    if (*A.bad) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) raise_status(A.status, DEV_ERR_INPUT);
+        return;
+    }
     const int tot = A.p + A.q; // work items: k reduced points + p columns + q rows
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot + A.k; t += gridDim.x * blockDim.x) {
         if (t < A.k) {
@@ -1601,10 +1691,6 @@ __global__ void __launch_bounds__(256) direct_sum_kernel(const int32_t *P, const
 
 inline int blocks_for(long n, int threads) { return int(std::min<long>((n + threads - 1) / threads, 148L * 16)); }
 
-__global__ void report_bad_kernel(const int32_t *bad, uint32_t *status)
-{
-    if (*bad) raise_status(status, DEV_ERR_INPUT);
-}
 
 } // namespace
 
@@ -1707,8 +1793,8 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     int32_t *Q_c2r = reinterpret_cast<int32_t *>(take(size_t(q) * 4));
     int32_t *map_row = reinterpret_cast<int32_t *>(take(kk * 4));
     int32_t *map_col = reinterpret_cast<int32_t *>(take(kk * 4));
-    // Error flag, then the fused partitions' tile words (one per tile and
-    // level), their done flags and tickets (one per level): zeroed by one
+    // Error flag, then the partitions' tile words (one per tile and level),
+    // their done flags, the ticket and the levels' done counts: zeroed by one
     // memset.
     const int lc = cutoff_level(k, cutoff); // first level whose nodes fit a block
     const int part_bs = part_threads(k) * PART_PER;
@@ -1719,36 +1805,34 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     int32_t *bad = reinterpret_cast<int32_t *>(sync_area);
     unsigned long long *tiles = reinterpret_cast<unsigned long long *>(sync_area + 256);
     int32_t *done = reinterpret_cast<int32_t *>(sync_area + 256 + tile_words * 8);
-    int32_t *tickets = reinterpret_cast<int32_t *>(sync_area + 256 + tile_words * 12);
+    int32_t *ticket = reinterpret_cast<int32_t *>(sync_area + 256 + tile_words * 12);
+    int32_t *level_done = ticket + 1; // lc counts (lc <= 31 fits the last 256 bytes)
     const size_t tints = table_ints(k, cutoff);
     int32_t *tab_hi = reinterpret_cast<int32_t *>(take(2 * tints * 4)); // hi then lo counts of a level
     if (size_t(cur - static_cast<char *>(ws)) > ws_bytes) return fail(SLCS_ERR_ALLOC, "braid workspace too small");
 
     SLCS_CUDA(cudaMemsetAsync(sync_area, 0, sync_bytes, st));
-    SLCS_CUDA(cudaMemsetAsync(P_c2r, 0xff, size_t(p) * 4, st));
-    SLCS_CUDA(cudaMemsetAsync(Q_c2r, 0xff, size_t(q) * 4, st));
-    inverse_kernel<<<blocks_for(p, 256), 256, 0, st>>>(P, P_c2r, p, bad);
-    inverse_kernel<<<blocks_for(q, 256), 256, 0, st>>>(Q, Q_c2r, q, bad);
-    check_full_kernel<<<blocks_for(p, 256), 256, 0, st>>>(P_c2r, p, bad);
-    check_full_kernel<<<blocks_for(q, 256), 256, 0, st>>>(Q_c2r, q, bad);
-    int32_t *Pcur = PQ, *Qcur = PQ + kk, *Pnext = PQ + 2 * kk, *Qnext = PQ + 3 * kk;
+    inverse_pair_kernel<<<blocks_for(long(p) + q, 256), 256, 0, st>>>(P, P_c2r, p, Q, Q_c2r, q, bad);
+    int32_t *Pcur = PQ, *Qcur = PQ + kk;
     {
-        SliceArgs S{P, Q_c2r, p, q, k, row_glue ? 0 : p - k, row_glue ? q - k : 0, Pcur, Qcur, map_row, map_col,
-                    scanP, scanQ, bsP, bsQ, n, bad};
+        SliceArgs S{P, Q_c2r, P_c2r, Q, p, q, k, row_glue ? 0 : p - k, row_glue ? q - k : 0, Pcur, Qcur, map_row,
+                    map_col, scanP, scanQ, bsP, bsQ, n, bad};
         slice_count_kernel<<<nbs, 256, 0, st>>>(S);
         part_bsum_kernel<<<1, 1024, 0, st>>>(bsP, bsQ, nbs);
         slice_write_kernel<<<nbs, 256, 0, st>>>(S);
     }
-    // Levels above the cutoff: device-wide partitions, one fused launch each.
-    for (int l = 0; l < lc; ++l) {
-        LevelArgs A{Pcur, Qcur, Pnext, Qnext, maps + 2 * kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1) + kk,
-                    scanP, scanQ, bsP, bsQ, k, l, bad};
-        FusedArgs F{A, tiles + size_t(l) * size_t(kb), done + size_t(l) * size_t(kb), tickets + l, bad,
-                    device_status_word()};
-        if (part_threads(k) == 1024) part_fused_kernel<1024><<<kb, 1024, 0, st>>>(F);
-        else part_fused_kernel<256><<<kb, 256, 0, st>>>(F);
-        std::swap(Pcur, Pnext);
-        std::swap(Qcur, Qnext);
+    // Levels above the cutoff: device-wide partitions, all in one launch
+    // (level l reads the even or odd pair of PQ's arrays and writes the other).
+    if (lc > 0) {
+        PartAllArgs G{PQ, maps, scanP, scanQ, k, lc, kb, tiles, done, ticket, level_done, bad, device_status_word()};
+        const int threads = part_threads(k);
+        const long grid = std::min<long>(long(lc) * kb, long(sm_count()) * (2048 / threads));
+        if (threads == 1024) part_levels_kernel<1024><<<int(grid), 1024, 0, st>>>(G);
+        else part_levels_kernel<256><<<int(grid), 256, 0, st>>>(G);
+        if (lc & 1) {
+            Pcur = PQ + 2 * kk;
+            Qcur = PQ + 3 * kk;
+        }
     }
     // Nodes of level lc: one block each, down to the leaves and back.
     {
@@ -1797,9 +1881,8 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
             walk_segments_kernel<<<int((warps * 32 + 127) / 128), 128, wsm, st>>>(SA, nodes);
         }
     }
-    AssembleArgs A{P, P_c2r, Q, res, map_row, map_col, out, p, q, k, row_glue, bad};
+    AssembleArgs A{P, P_c2r, Q, res, map_row, map_col, out, p, q, k, row_glue, bad, device_status_word()};
     assemble_kernel<<<blocks_for(long(p) + q + k, 256), 256, 0, st>>>(A);
-    report_bad_kernel<<<1, 1, 0, st>>>(bad, device_status_word());
     SLCS_CUDA(cudaGetLastError());
     return SLCS_OK;
 }
