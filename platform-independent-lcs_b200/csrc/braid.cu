@@ -1016,11 +1016,19 @@ struct GlueArgs {
     // glued: (G+1)^2 per node and table, G = node size / B.
     int32_t *cnt_hi, *cnt_lo;
     int B, stride;
+    // The next level's tables: the other of the two table buffers, free since
+    // the walk one level down read it; zeroed here for that level's glue
+    // (instead of a memset launch per level).
+    int32_t *clear;
+    long long nclear;
 };
 
 __global__ void __launch_bounds__(256) glue_kernel(GlueArgs A)
 {
     if (*A.bad) return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < A.nclear;
+         i += (long long)gridDim.x * blockDim.x)
+        A.clear[i] = 0;
     const bool pow2 = (A.k & (A.k - 1)) == 0;
     int lg = 0; // log2 k for a power of two
     while (pow2 && (1 << lg) < A.k) ++lg;
@@ -1737,7 +1745,7 @@ slcs_status braid_workspace_bytes(int p, int q, int k, int cutoff, size_t *bytes
     if (cutoff <= 0) cutoff = 1024;
     if (cutoff > SUB_MAX) cutoff = SUB_MAX;
     size_t b = 0;
-    b += 2 * table_ints(k, cutoff) * sizeof(int32_t) + 512; // delta tables (hi, lo)
+    b += 4 * table_ints(k, cutoff) * sizeof(int32_t) + 512; // delta tables (hi, lo), two buffers
     b += 4 * kk * sizeof(int32_t);                         // P/Q ping-pong
     b += 2 * kk * size_t(levels + 2) * sizeof(int32_t);    // maps per level
     b += kk * size_t(levels + 2) * sizeof(int32_t);        // results per level
@@ -1808,10 +1816,24 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     int32_t *ticket = reinterpret_cast<int32_t *>(sync_area + 256 + tile_words * 12);
     int32_t *level_done = ticket + 1; // lc counts (lc <= 31 fits the last 256 bytes)
     const size_t tints = table_ints(k, cutoff);
-    int32_t *tab_hi = reinterpret_cast<int32_t *>(take(2 * tints * 4)); // hi then lo counts of a level
+    // Two table buffers, each a level's hi then lo counts; levels alternate.
+    int32_t *tabs = reinterpret_cast<int32_t *>(take(4 * tints * 4));
     if (size_t(cur - static_cast<char *>(ws)) > ws_bytes) return fail(SLCS_ERR_ALLOC, "braid workspace too small");
 
+    // Level l's tables: entries of each of the two, and place in the buffer
+    // of its parity.
+    auto level_tables = [&](int l, size_t *tentries) {
+        int B, stride;
+        walk_grid(k, l, B, stride);
+        *tentries = (size_t(1) << l) * size_t(stride) * size_t(stride);
+        return tabs + size_t(l & 1) * 2 * tints;
+    };
     SLCS_CUDA(cudaMemsetAsync(sync_area, 0, sync_bytes, st));
+    if (lc > 0) { // the deepest level's tables; each level's glue clears the next level's
+        size_t te = 0;
+        int32_t *t0 = level_tables(lc - 1, &te);
+        SLCS_CUDA(cudaMemsetAsync(t0, 0, 2 * te * sizeof(int32_t), st));
+    }
     inverse_pair_kernel<<<blocks_for(long(p) + q, 256), 256, 0, st>>>(P, P_c2r, p, Q, Q_c2r, q, bad);
     int32_t *Pcur = PQ, *Qcur = PQ + kk;
     {
@@ -1850,13 +1872,16 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
         int B, stride;
         walk_grid(k, l, B, stride);
         const int nodes = 1 << l;
-        const size_t tentries = size_t(nodes) * stride * stride;
-        // hi and lo counts of the level side by side: one clear for both,
-        // filled by the glue as it places the points
+        // hi and lo counts of the level side by side (zeroed by the memset
+        // above or by the glue one level down), filled by the glue as it
+        // places the points
+        size_t tentries = 0, next_entries = 0;
+        int32_t *tab_hi = level_tables(l, &tentries);
         int32_t *lvl_lo = tab_hi + tentries;
-        SLCS_CUDA(cudaMemsetAsync(tab_hi, 0, 2 * tentries * sizeof(int32_t), st));
+        int32_t *next = l > 0 ? level_tables(l - 1, &next_entries) : nullptr;
         GlueArgs G{res + kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1), maps + 2 * kk * size_t(l + 1) + kk,
-                   C, Rr, res + kk * size_t(l), k, l, bad, tab_hi, lvl_lo, B, stride};
+                   C, Rr, res + kk * size_t(l), k, l, bad, tab_hi, lvl_lo, B, stride, next,
+                   (long long)(2 * next_entries)};
         glue_kernel<<<blocks_for(k, 256), 256, 0, st>>>(G);
         TableArgs TA{C, tab_hi, lvl_lo, k, l, B, stride, bad};
         if (size_t(stride) * stride <= size_t(SMALL_TABLE)) {
