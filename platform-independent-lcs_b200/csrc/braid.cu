@@ -191,10 +191,12 @@ struct PartAllArgs {
     int32_t *maps;             // level l + 1's pmap at maps + 2k(l + 1), its qmap k further
     int32_t *scanP, *scanQ;
     int k, levels, kb;         // levels above the cutoff, tiles per level
+    bool pow2;                 // k is a power of two: node boundaries are multiples of the node size
     unsigned long long *tiles; // levels * kb tile status words, zero at launch
     int32_t *done;             // levels * kb scan-written flags, zero at launch
     int32_t *ticket;           // zero at launch
     int32_t *level_done;       // per level: tiles scattered, zero at launch
+    int32_t *scat;             // levels * kb: the tile has scattered (1), zero at launch
     int32_t *err;
     uint32_t *status;
 };
@@ -229,7 +231,7 @@ struct PartSmem {
 // One tile of one level: count, look back, scan, scatter.  False when the
 // product failed (err raised here or elsewhere); the block then stops.
 template <int PART_THREADS>
-__device__ __forceinline__ bool part_tile(const FusedArgs &F, int tile, PartSmem<PART_THREADS> &S)
+__device__ __forceinline__ bool part_tile(const FusedArgs &F, int tile, bool local, PartSmem<PART_THREADS> &S)
 {
     const LevelArgs &A = F.L;
     constexpr int PER = PART_PER;
@@ -304,7 +306,10 @@ __device__ __forceinline__ bool part_tile(const FusedArgs &F, int tile, PartSmem
         }
         int ep = 0, eq = 0;
         bool ok = true;
-        if (tile == 0) {
+        if (local) {
+            // Every node of the level lies inside one tile: node-relative
+            // counts need only the tile's own scan (no look-back).
+        } else if (tile == 0) {
             if (lane == 0) st_release_u64(F.tiles, pack_counts(TILE_INCL, tp, tq));
         } else {
             if (lane == 0) st_release_u64(F.tiles + tile, pack_counts(TILE_AGG, tp, tq));
@@ -429,25 +434,40 @@ __global__ void __launch_bounds__(PART_THREADS) part_levels_kernel(PartAllArgs G
         if (threadIdx.x == 0) {
             s_ticket = atomicAdd(G.ticket, 1);
             S.s_ok = !ld_relaxed_gpu(G.err);
-            const int lv = s_ticket / G.kb;
+            const int lv = s_ticket / G.kb, tl = s_ticket % G.kb;
             if (S.s_ok && lv > 0 && lv < G.levels) {
-                // every tile of the level above has scattered into this level's input
-                uint64_t t0 = 0;
-                while (ld_acquire_gpu(G.level_done + lv - 1) < G.kb) {
-                    if (ld_relaxed_gpu(G.err)) {
-                        S.s_ok = 0;
-                        break;
+                // This tile's input is written by the tiles of the level above
+                // that hold a node overlapping the tile: when the parent nodes
+                // are at most two tiles long (power-of-two k), those tiles
+                // only; otherwise every tile of the level.
+                const int ps = G.k >> (lv - 1); // parent node size (power-of-two k)
+                const bool near = G.pow2 && ps <= 2 * PART_BS;
+                const int32_t *ctr = G.level_done + lv - 1;
+                int want = G.kb, ta = 0, tb = 0;
+                if (near) {
+                    ta = (tl * PART_BS) / ps * ps / PART_BS;
+                    tb = min(G.kb - 1, ((tl * PART_BS + PART_BS - 1) / ps * ps + ps - 1) / PART_BS);
+                    want = 1;
+                }
+                for (int u = ta; u <= tb && S.s_ok; ++u) {
+                    if (near) ctr = G.scat + size_t(lv - 1) * G.kb + u;
+                    uint64_t t0 = 0;
+                    while (ld_acquire_gpu(ctr) < want) {
+                        if (ld_relaxed_gpu(G.err)) {
+                            S.s_ok = 0;
+                            break;
+                        }
+                        const uint64_t now = globaltimer_ns();
+                        if (t0 == 0) {
+                            t0 = now;
+                        } else if (now - t0 > PART_WAIT_NS) {
+                            atomicExch(G.err, 1);
+                            raise_status(G.status, DEV_ERR_TIMEOUT);
+                            S.s_ok = 0;
+                            break;
+                        }
+                        __nanosleep(64);
                     }
-                    const uint64_t now = globaltimer_ns();
-                    if (t0 == 0) {
-                        t0 = now;
-                    } else if (now - t0 > PART_WAIT_NS) {
-                        atomicExch(G.err, 1);
-                        raise_status(G.status, DEV_ERR_TIMEOUT);
-                        S.s_ok = 0;
-                        break;
-                    }
-                    __nanosleep(64);
                 }
             }
         }
@@ -460,11 +480,12 @@ __global__ void __launch_bounds__(PART_THREADS) part_levels_kernel(PartAllArgs G
         FusedArgs F{LevelArgs{in, in + kk, nx, nx + kk, mp, mp + kk, G.scanP, G.scanQ, nullptr, nullptr, G.k, lv,
                               G.err},
                     G.tiles + size_t(lv) * G.kb, G.done + size_t(lv) * G.kb, G.err, G.status};
-        if (!part_tile<PART_THREADS>(F, tile, S)) return;
-        (void)PART_BS;
+        const bool local = G.pow2 && (G.k >> lv) <= PART_BS; // the level's nodes fit inside tiles
+        if (!part_tile<PART_THREADS>(F, tile, local, S)) return;
         __syncthreads(); // every thread of the tile has scattered
         if (threadIdx.x == 0) {
             __threadfence();
+            st_release_gpu(G.scat + size_t(lv) * G.kb + tile, 1);
             atomicAdd(G.level_done + lv, 1);
         }
     }
@@ -1755,7 +1776,7 @@ slcs_status braid_workspace_bytes(int p, int q, int k, int cutoff, size_t *bytes
     b += size_t(p) * sizeof(int32_t) + size_t(q) * sizeof(int32_t); // inverses
     b += 2 * kk * sizeof(int32_t);                         // map_row, map_col
     b += 64 * 256 + 256;                                    // alignment slack, flag
-    b += size_t(levels + 1) * ((size_t(std::max(k, 1)) + 256 * PART_PER - 1) / (256 * PART_PER)) * 12 + 512; // partition tiles
+    b += size_t(levels + 1) * ((size_t(std::max(k, 1)) + 256 * PART_PER - 1) / (256 * PART_PER)) * 16 + 512; // partition tiles
     *bytes = b;
     return SLCS_OK;
 }
@@ -1808,13 +1829,14 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     const int part_bs = part_threads(k) * PART_PER;
     const int kb = int((kk + part_bs - 1) / part_bs);
     const size_t tile_words = size_t(lc) * size_t(kb);
-    const size_t sync_bytes = 256 + tile_words * 8 + tile_words * 4 + 256;
+    const size_t sync_bytes = 256 + tile_words * 8 + tile_words * 4 + 256 + tile_words * 4;
     char *sync_area = take(sync_bytes);
     int32_t *bad = reinterpret_cast<int32_t *>(sync_area);
     unsigned long long *tiles = reinterpret_cast<unsigned long long *>(sync_area + 256);
     int32_t *done = reinterpret_cast<int32_t *>(sync_area + 256 + tile_words * 8);
     int32_t *ticket = reinterpret_cast<int32_t *>(sync_area + 256 + tile_words * 12);
-    int32_t *level_done = ticket + 1; // lc counts (lc <= 31 fits the last 256 bytes)
+    int32_t *level_done = ticket + 1; // lc counts (lc <= 31 fits these 256 bytes)
+    int32_t *scat = reinterpret_cast<int32_t *>(sync_area + 256 + tile_words * 12 + 256);
     const size_t tints = table_ints(k, cutoff);
     // Two table buffers, each a level's hi then lo counts; levels alternate.
     int32_t *tabs = reinterpret_cast<int32_t *>(take(4 * tints * 4));
@@ -1846,7 +1868,8 @@ slcs_status launch_braid(const int32_t *P, int p, const int32_t *Q, int q, int k
     // Levels above the cutoff: device-wide partitions, all in one launch
     // (level l reads the even or odd pair of PQ's arrays and writes the other).
     if (lc > 0) {
-        PartAllArgs G{PQ, maps, scanP, scanQ, k, lc, kb, tiles, done, ticket, level_done, bad, device_status_word()};
+        PartAllArgs G{PQ, maps, scanP, scanQ, k, lc, kb, (k & (k - 1)) == 0, tiles, done, ticket, level_done, scat,
+                      bad, device_status_word()};
         const int threads = part_threads(k);
         const long grid = std::min<long>(long(lc) * kb, long(sm_count()) * (2048 / threads));
         if (threads == 1024) part_levels_kernel<1024><<<int(grid), 1024, 0, st>>>(G);
