@@ -62,6 +62,15 @@ def test_large_merge(cuda):
         _check(P, Q, m, False, cuda, cutoff)
 
 
+@pytest.mark.parametrize("k,cutoff,glue", [(1 << 20, 256, False), (1 << 20, 1024, True), (300001, 256, True),
+                                            (600000, 64, False)])
+def test_large_random_products(cuda, k, cutoff, glue):
+    """Overlaps whose top levels walk in warp segments split into parts
+    (grid spacing above 256): power-of-two and other k, both glues."""
+    rng = np.random.default_rng(k + cutoff)
+    _check(rng.permutation(k + 1000), rng.permutation(k + 3000), k, glue, cuda, cutoff)
+
+
 def test_small_and_edge_sizes(cuda):
     rng = np.random.default_rng(5)
     for (p, q, k) in [(1, 1, 0), (1, 1, 1), (2, 1, 1), (1, 2, 1), (2, 2, 2), (3, 5, 3), (5, 3, 0), (17, 17, 17)]:
