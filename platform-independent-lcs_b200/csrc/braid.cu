@@ -11,10 +11,12 @@
 //     the node containing entry i at level l follows from i alone (node_of).
 //   * Downward, each level is a stable partition of every node: P's rows by
 //     column < s/2 (get_vert_slice, 5-19) and Q's columns by row < s/2
-//     (get_horz_slice, 22-36).  Above the cutoff the partition is one
-//     single-pass launch per level (tiles publish their counts and look back
-//     over their predecessors, every wait bounded); the maps from child index
-//     to parent index are kept per level.
+//     (get_horz_slice, 22-36).  Above the cutoff every level's partition runs
+//     in one launch: single-pass tiles (they publish their counts and look
+//     back over their predecessors) take tickets level by level, and a tile
+//     first waits for the tiles of the level above that hold its parent
+//     nodes; every wait is bounded.  The maps from child index to parent
+//     index are kept per level.
 //   * A node at or below the cutoff is finished by one thread block: it loads
 //     the node into shared memory (16-bit local indices) and runs every lower
 //     level of its subtree there, down and back up, with block-wide scans.
