@@ -314,8 +314,9 @@ static slcs_status write_identity(int32_t *h, int32_t m, int32_t *v, int32_t n, 
 using namespace slcs;
 
 struct StreamClass {
-    int tm, seg;
+    int tm, seg;  // rows per lane, lanes per segment
     bool packed;
+    bool var = false; // a lane count of the variable packed class (segments share warps)
 };
 
 // Relative time of one step of a warp of a stream class (all its segments
@@ -343,10 +344,9 @@ static double class_step_time(const StreamClass &k, int tns)
 }
 
 // Head of a batch plan's work buffer: counters [0] wavefront ticket and [1]
-// abort, [2..3] unused, then MAX_CLASSES pool tickets (rounded up to 16);
+// abort, [2..3] unused, then MAX_POOLS pool tickets;
 // the wavefront progress counters follow.
-static constexpr int WORK_HEAD = 4 + 16;
-static_assert(MAX_CLASSES <= 16, "pool tickets of every class fit the work head");
+static constexpr int WORK_HEAD = 4 + MAX_POOLS;
 
 struct slcs_batch_plan {
     int device = 0;
@@ -364,6 +364,9 @@ struct slcs_batch_plan {
     int32_t nclass = 0; // classes with warps
     int32_t class_warp_end[MAX_CLASSES] = {};
     int32_t class_code[MAX_CLASSES] = {};
+    int32_t class_pool[MAX_CLASSES] = {};
+    std::vector<int32_t> lane_map; // the variable class's warps: 32 entries each (BatchLaunch::lane_map)
+    int32_t *d_lane_map = nullptr;
     int32_t nwarps = 0; // warps with a stream class
     int grid = 0;       // blocks of the batch launch
     uint64_t wait_ns = DEFAULT_WAIT_NS;
@@ -374,7 +377,7 @@ struct slcs_batch_plan {
     int32_t *d_seg_list2 = nullptr;
     int32_t *d_pool_list = nullptr;
     int32_t *d_pool_list2 = nullptr;
-    int32_t pool_off[MAX_CLASSES + 1] = {};
+    int32_t pool_off[MAX_POOLS + 1] = {};
     int pool_pct = 15;
     int2 *d_tasks = nullptr;
     int64_t *d_scr_off = nullptr;
@@ -433,11 +436,13 @@ struct slcs_batch_plan {
             for (int c = 0; c < nclass; ++c) {
                 B.class_warp_end[c] = class_warp_end[c];
                 B.class_code[c] = class_code[c];
+                B.class_pool[c] = class_pool[c];
             }
+            B.lane_map = d_lane_map;
             B.pool_list = d_pool_list;
             B.pool_list2 = d_pool_list2;
             B.pool_ticket = d_work + 4;
-            for (int c = 0; c <= MAX_CLASSES; ++c) B.pool_off[c] = pool_off[c];
+            for (int c = 0; c <= MAX_POOLS; ++c) B.pool_off[c] = pool_off[c];
             s = launch_batch(B, tns, st, nullptr);
         } else {
             s = launch_comb(launch(a, b, out), tm, warps, st, nullptr);
@@ -831,27 +836,37 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
         } else {
             P->stm = 16;
             P->seg = 16;
+            // Packed pairs: the variable class, one item class per lane count
+            // (16 rows per lane, segments of VAR_MIN_LANES..32 lanes side by
+            // side in a warp), so that a pair's rows are padded to a multiple
+            // of 16 rather than to one of a few class heights.
             if (pack)
-                for (int t : {4, 8, 12, 16}) P->classes.push_back({t, 16, true});
+                for (int l = VAR_MIN_LANES; l <= 32; ++l) P->classes.push_back({VAR_TM, l, true, true});
             for (int t : {4, 8, 12, 16}) P->classes.push_back({t, 16, false});
             P->classes.push_back({12, 32, false});
             P->classes.push_back({16, 32, false});
         }
         for (const auto &c : P->classes)
-            if (c.packed ? !packed16_supported(c.tm, c.seg) : !stream_variant_supported(c.tm, c.seg)) {
+            if (!c.var && (c.packed ? !packed16_supported(c.tm, c.seg) : !stream_variant_supported(c.tm, c.seg))) {
                 delete P;
                 return fail(SLCS_ERR_UNSUPPORTED, "stream mode needs tile_m in {4,8,12,16} and seg in {8,16,32}");
             }
-        // Packed plans: 8 warps per SM and half of each class's work in its
-        // pool.  A packed item is a couple of pairs, and with 16 warps per SM
-        // a segment combed only one or two of them, so the launch ended with
-        // whichever segments drew two; at 8 warps per SM each warp runs
-        // twice as fast and combs twice as many items (20,000 reads on B200:
-        // 0.381 -> 0.328 ms).  32-bit plans keep the full occupancy (2 blocks
-        // per SM: 0.361 -> 0.420 ms) and a 15 % pool.
+        // Packed plans: half of each class's work in its pool.  Fixed packed
+        // classes (16-lane segments) run 8 warps per SM: a packed item is a
+        // couple of pairs, and with 16 warps per SM a segment combed only one
+        // or two of them, so the launch ended with whichever segments drew
+        // two; at 8 warps per SM each warp runs twice as fast and combs twice
+        // as many items (20,000 reads on B200: 0.381 -> 0.328 ms).  The
+        // variable class keeps the full occupancy: its segments are as short
+        // as their pairs allow, so many more of them run side by side
+        // (0.340 ms at 8 warps per SM, 0.318 ms at 16).  32-bit plans keep
+        // the full occupancy too (2 blocks per SM: 0.361 -> 0.420 ms) and a
+        // 15 % pool.
         const bool packed_plan = pack && std::any_of(P->classes.begin(), P->classes.end(),
                                                      [](const StreamClass &k) { return k.packed; });
-        P->blocks_per_sm = (cfg && cfg->blocks_per_sm > 0) ? cfg->blocks_per_sm : (packed_plan ? 2 : 0);
+        const bool var_plan = std::any_of(P->classes.begin(), P->classes.end(),
+                                          [](const StreamClass &k) { return k.var; });
+        P->blocks_per_sm = (cfg && cfg->blocks_per_sm > 0) ? cfg->blocks_per_sm : (packed_plan && !var_plan ? 2 : 0);
         P->pool_pct = packed_plan ? 50 : 15;
         if (cfg && cfg->pool_pct != 0) P->pool_pct = cfg->pool_pct < 0 ? 0 : std::min(cfg->pool_pct, 90);
     }
@@ -924,26 +939,28 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
             const int32_t n = std::max(pairs[it.first].n, it.second >= 0 ? pairs[it.second].n : 0);
             return int64_t((n + cols - 1) / cols) + 2;
         };
-        // Per class: its steps in total, its longest item, and how many warps
-        // can have work at all.
+        // Per class: its steps in total, its longest item, and how many units
+        // can have work at all.  A unit is a warp of a fixed class (32 / seg
+        // segments) or one segment of the variable class (its lane count).
         std::vector<double> csteps(nclass, 0.0), clong(nclass, 0.0);
-        std::vector<long> wmax(nclass, 0);
+        std::vector<long> umax(nclass, 0);
+        auto unit_lanes = [&](int c) { return P->classes[c].var ? P->classes[c].seg : 32; };
+        auto unit_segs = [&](int c) { return P->classes[c].var ? 1 : 32 / P->classes[c].seg; };
         for (int c = 0; c < nclass; ++c) {
             int64_t w = 0, longest = 0;
             for (const auto &it : items[c]) {
                 w += cost(c, it);
                 longest = std::max(longest, cost(c, it));
             }
-            const int spw = 32 / P->classes[c].seg;
             csteps[c] = double(w);
             clong[c] = double(longest);
-            wmax[c] = (long(items[c].size()) + spw - 1) / spw;
+            umax[c] = (long(items[c].size()) + unit_segs(c) - 1) / unit_segs(c);
         }
         const long want_wf = (long(P->ntasks) + BATCH_WARPS - 1) / BATCH_WARPS;
         long want = std::max<long>(1, want_wf);
-        long sum_wmax = 0;
-        for (int c = 0; c < nclass; ++c) sum_wmax += wmax[c];
-        want = std::max(want, (sum_wmax + BATCH_WARPS - 1) / BATCH_WARPS);
+        long lanes_max = 0;
+        for (int c = 0; c < nclass; ++c) lanes_max += umax[c] * unit_lanes(c);
+        want = std::max(want, (lanes_max / 32 + 1 + BATCH_WARPS - 1) / BATCH_WARPS);
         grid = int(std::max<long>(1, std::min<long>(grid, want)));
         // One warp per wavefront task gets no stream list: those warps take
         // the tasks from the start, so the stripe chains of the tall pairs
@@ -952,53 +969,156 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
         // the 20,000-read launch).
         const long reserve = std::min<long>(P->ntasks, long(grid) * BATCH_WARPS / 8);
         const long warps_total = long(grid) * BATCH_WARPS - reserve;
-        // Warps per class so that the classes end together.  A class of w
-        // warps ends about when each of its w * spw segments has combed its
-        // share of the class's steps and the last one its longest item, half
-        // of which is still to go on average: end(w) = t * (S / (w * spw) +
-        // L / 2), t the class's time per step.  Each warp goes to the class
-        // that would end last.  (Shares in proportion to S * t alone gave the
-        // 385-512-row class of the 20,000 reads 30 warps for 64 items of
-        // ~150 steps: it ended ~40 us after every other class.)
-        std::vector<long> wc(nclass, 0);
-        long used = 0;
-        auto class_end = [&](int c, long w) {
-            const int spw = 32 / P->classes[c].seg;
-            return class_step_time(P->classes[c], P->tns) * (csteps[c] / double(w * spw) + clong[c] / 2.0);
+        // Units per class so that the classes end together.  A class of u
+        // units ends about when each of its segments has combed its share of
+        // the class's steps and the last one its longest item, half of which
+        // is still to go on average: end(u) = t * (S / (u * segments per
+        // unit) + L / 2), t the class's time per step.  Each unit goes to the
+        // class that would end last, while the lanes last.  (Shares in
+        // proportion to S * t alone gave the 385-512-row class of the 20,000
+        // reads 30 warps for 64 items of ~150 steps: it ended ~40 us after
+        // every other class.)
+        std::vector<long> uc(nclass, 0);
+        auto class_end = [&](int c, long u) {
+            return class_step_time(P->classes[c], P->tns) * (csteps[c] / double(u * unit_segs(c)) + clong[c] / 2.0);
         };
+        // Warps the variable class's segments need, packed first fit
+        // (largest first); layout[w] lists (class, lanes) of warp w.
+        std::vector<std::vector<std::pair<int, int>>> layout;
+        auto pack_var = [&]() {
+            std::vector<std::pair<int, int>> segs; // (lanes, class)
+            for (int c = 0; c < nclass; ++c)
+                if (P->classes[c].var)
+                    for (long u = 0; u < uc[c]; ++u) segs.push_back({P->classes[c].seg, c});
+            std::stable_sort(segs.begin(), segs.end(), [](const std::pair<int, int> &x, const std::pair<int, int> &y) {
+                return x.first > y.first;
+            });
+            layout.clear();
+            std::vector<int> room;
+            for (const auto &sg : segs) {
+                size_t w = 0;
+                while (w < room.size() && room[w] < sg.first) ++w;
+                if (w == room.size()) {
+                    room.push_back(32);
+                    layout.emplace_back();
+                }
+                room[w] -= sg.first;
+                layout[w].push_back({sg.second, sg.first});
+            }
+            return long(layout.size());
+        };
+        auto warps_needed = [&]() {
+            long w = pack_var();
+            for (int c = 0; c < nclass; ++c)
+                if (!P->classes[c].var) w += uc[c];
+            return w;
+        };
+        long lanes_used = 0;
         for (int c = 0; c < nclass; ++c) {
             if (items[c].empty()) continue;
-            wc[c] = 1;
-            ++used;
+            uc[c] = 1;
+            lanes_used += unit_lanes(c);
         }
-        while (used < warps_total) {
+        for (;;) {
             int worst = -1;
             double worst_end = -1.0;
             for (int c = 0; c < nclass; ++c) {
-                if (wc[c] == 0 || wc[c] >= wmax[c]) continue;
-                const double e = class_end(c, wc[c]);
+                if (uc[c] == 0 || uc[c] >= umax[c] || lanes_used + unit_lanes(c) > warps_total * 32) continue;
+                const double e = class_end(c, uc[c]);
                 if (e > worst_end) {
                     worst_end = e;
                     worst = c;
                 }
             }
-            if (worst < 0) break; // every class has a warp per item
-            ++wc[worst];
-            ++used;
+            if (worst < 0) break; // out of lanes, or every class has a unit per item
+            ++uc[worst];
+            lanes_used += unit_lanes(worst);
         }
-        if (std::count_if(wc.begin(), wc.end(), [](long w) { return w > 0; }) > MAX_CLASSES) {
+        // Packing loses a few lanes: take units back from the classes that
+        // end first until the warps fit.
+        for (long need = warps_needed(); need > warps_total; need = warps_needed()) {
+            int best = -1;
+            double best_end = 0.0;
+            for (int c = 0; c < nclass; ++c) {
+                if (uc[c] <= 1) continue;
+                const double e = class_end(c, uc[c] - 1);
+                if (best < 0 || e < best_end) {
+                    best_end = e;
+                    best = c;
+                }
+            }
+            if (best < 0) break;
+            --uc[best];
+        }
+        const long var_warps = pack_var();
+        long used = var_warps;
+        int nfixed = 0;
+        for (int c = 0; c < nclass; ++c)
+            if (!P->classes[c].var && uc[c] > 0) {
+                used += uc[c];
+                ++nfixed;
+            }
+        int npools = 0;
+        for (int c = 0; c < nclass; ++c) npools += uc[c] > 0;
+        if (nfixed + (var_warps > 0) > MAX_CLASSES || npools > MAX_POOLS) {
             delete P;
             return fail(SLCS_ERR_UNSUPPORTED, "too many stream classes in use");
         }
         P->grid = int(std::max<long>(grid, (used + BATCH_WARPS - 1) / BATCH_WARPS));
         P->nclass = 0;
-        long wbase = 0;
         std::vector<std::vector<std::pair<int32_t, int32_t>>> slot_lists(size_t(std::max(used, 1L)) * SEG_SLOTS);
         std::vector<std::pair<int32_t, int32_t>> pool_items;
-        for (int c = 0; c < nclass; ++c) {
-            if (wc[c] == 0) continue;
-            const int spw = 32 / P->classes[c].seg;
-            const long nseg = wc[c] * spw;
+        // Segments of every class, as global slot ids (SEG_SLOTS * warp + slot).
+        std::vector<std::vector<long>> class_slots(nclass);
+        std::vector<int> class_pool_of(nclass, -1);
+        if (var_warps > 0) {
+            P->lane_map.assign(size_t(var_warps) * 32, -1);
+            int next_pool = 0;
+            for (int c = 0; c < nclass; ++c)
+                if (P->classes[c].var && uc[c] > 0) class_pool_of[c] = next_pool++;
+            for (long w = 0; w < var_warps; ++w) {
+                int lane0 = 0;
+                for (size_t j = 0; j < layout[w].size(); ++j) {
+                    const int c = layout[w][j].first, nl = layout[w][j].second;
+                    class_slots[c].push_back(long(w) * SEG_SLOTS + long(j));
+                    for (int l = 0; l < nl; ++l)
+                        P->lane_map[size_t(w) * 32 + size_t(lane0 + l)] =
+                            (class_pool_of[c] << 24) | (int(j) << 16) | (l << 8) | nl;
+                    lane0 += nl;
+                }
+            }
+            P->class_warp_end[P->nclass] = int32_t(var_warps);
+            P->class_code[P->nclass] = PACKED16_VAR_CODE + VAR_TM * 100;
+            P->class_pool[P->nclass] = -1;
+            ++P->nclass;
+        }
+        {
+            int next_pool = 0;
+            for (int c = 0; c < nclass; ++c)
+                if (class_pool_of[c] >= 0) next_pool = std::max(next_pool, class_pool_of[c] + 1);
+            long wbase = var_warps;
+            for (int c = 0; c < nclass; ++c) {
+                if (P->classes[c].var || uc[c] == 0) continue;
+                const int spw = 32 / P->classes[c].seg;
+                for (long u = 0; u < uc[c]; ++u)
+                    for (int j = 0; j < spw; ++j) class_slots[c].push_back((wbase + u) * SEG_SLOTS + j);
+                wbase += uc[c];
+                class_pool_of[c] = next_pool++;
+                P->class_warp_end[P->nclass] = int32_t(wbase);
+                P->class_code[P->nclass] = P->classes[c].tm * 100 + P->classes[c].seg +
+                                           (P->classes[c].packed ? PACKED16_CODE : 0);
+                P->class_pool[P->nclass] = class_pool_of[c];
+                ++P->nclass;
+            }
+        }
+        // Lists and pools, pool by pool.
+        std::vector<int> by_pool(npools, -1);
+        for (int c = 0; c < nclass; ++c)
+            if (class_pool_of[c] >= 0) by_pool[class_pool_of[c]] = c;
+        for (int pi = 0; pi < npools; ++pi) {
+            const int c = by_pool[pi];
+            const auto &slots = class_slots[c];
+            const long nseg = long(slots.size());
             using Load = std::pair<int64_t, int64_t>;
             std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
             for (long sgi = 0; sgi < nseg; ++sgi) heap.push({0, sgi});
@@ -1014,7 +1134,7 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
             int64_t class_cost = 0;
             for (const auto &it : items[c]) class_cost += cost(c, it);
             const double cap = (100 - P->pool_pct) / 100.0 * double(class_cost) / double(nseg);
-            P->pool_off[P->nclass] = int32_t(pool_items.size());
+            P->pool_off[pi] = int32_t(pool_items.size());
             for (const auto &it : items[c]) {
                 Load top = heap.top();
                 if (P->pool_pct > 0 && double(top.first) >= cap) {
@@ -1022,21 +1142,15 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
                     continue;
                 }
                 heap.pop();
-                const long warp = wbase + top.second / spw, sidx = top.second % spw;
-                slot_lists[size_t(warp) * SEG_SLOTS + size_t(sidx)].push_back(it);
+                slot_lists[size_t(slots[size_t(top.second)])].push_back(it);
                 top.first += cost(c, it);
                 heap.push(top);
             }
-            P->pool_off[P->nclass + 1] = int32_t(pool_items.size());
-            wbase += wc[c];
+            P->pool_off[pi + 1] = int32_t(pool_items.size());
             if (P->classes[c].packed) P->npacked += int32_t(cls_pairs[c].size());
-            P->class_warp_end[P->nclass] = int32_t(wbase);
-            P->class_code[P->nclass] = P->classes[c].tm * 100 + P->classes[c].seg +
-                                       (P->classes[c].packed ? PACKED16_CODE : 0);
-            ++P->nclass;
         }
-        P->nwarps = int32_t(wbase);
-        for (int c = P->nclass + 1; c <= MAX_CLASSES; ++c) P->pool_off[c] = P->pool_off[P->nclass];
+        P->nwarps = int32_t(used);
+        for (int pi = npools + 1; pi <= MAX_POOLS; ++pi) P->pool_off[pi] = P->pool_off[npools];
         for (const auto &it : pool_items) {
             pool_list.push_back(it.first);
             pool_list2.push_back(it.second);
@@ -1064,6 +1178,9 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
     alloc(reinterpret_cast<void **>(&P->d_seg_list2), sizeof(int32_t) * seg_list2.size());
     alloc(reinterpret_cast<void **>(&P->d_pool_list), sizeof(int32_t) * pool_list.size());
     alloc(reinterpret_cast<void **>(&P->d_pool_list2), sizeof(int32_t) * pool_list2.size());
+    alloc(reinterpret_cast<void **>(&P->d_lane_map), sizeof(int32_t) * P->lane_map.size());
+    if (e == cudaSuccess && !P->lane_map.empty())
+        e = cudaMemcpy(P->d_lane_map, P->lane_map.data(), sizeof(int32_t) * P->lane_map.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !pool_list.empty())
         e = cudaMemcpy(P->d_pool_list, pool_list.data(), sizeof(int32_t) * pool_list.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !pool_list2.empty())
@@ -1350,6 +1467,7 @@ slcs_status slcs_batch_plan_destroy(slcs_batch_plan *P)
     cudaFree(P->d_seg_list2);
     cudaFree(P->d_pool_list);
     cudaFree(P->d_pool_list2);
+    cudaFree(P->d_lane_map);
     cudaFree(P->d_tasks);
     cudaFree(P->d_scr_off);
     cudaFree(P->d_scratch);

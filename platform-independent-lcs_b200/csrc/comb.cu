@@ -446,6 +446,10 @@ struct ItemSource {
 
     __device__ __forceinline__ void pick(const BatchLaunch &B, int &pa, int &pb)
     {
+        if (cls < 0) { // an idle lane of a variable warp
+            pa = pb = -1;
+            return;
+        }
         const int off = B.pool_off[cls], size = B.pool_off[cls + 1] - off;
         if (q < count) {
             pa = la[q];
@@ -687,15 +691,21 @@ __device__ __forceinline__ uint32_t sym4(const uint8_t *b, int c, int n, bool &f
     return w;
 }
 
-template <int TM, int SEG>
-__device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int cls, int seg_id, int lane)
+// A segment of SEG lanes (lanes seg_lane0 .. seg_lane0 + SEG - 1 of the
+// warp; this lane is lane sl of it) streaming the items of pool `cls` (-1:
+// an idle lane, which only takes part in the warp's shuffles).  Segments of
+// any size may share a warp: a lane takes its neighbour's strands through a
+// full-warp shuffle, and the first lane of each segment replaces them with
+// the fresh ones of its column.
+template <int TM>
+__device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int cls, int seg_id, int lane, int sl,
+                                                 int SEG)
 {
     const CombLaunch &L = B.wf;
-    const int sl = lane & (SEG - 1);
     const int r0 = sl * TM;
-    const int seg_lane0 = lane & ~(SEG - 1);
-    const int beg = B.seg_off[seg_id];
-    ItemSource src{B.seg_list + beg, B.seg_list2 + beg, B.seg_off[seg_id + 1] - beg, 0, cls, -1};
+    const int seg_lane0 = lane - sl;
+    const int beg = cls < 0 ? 0 : B.seg_off[seg_id];
+    ItemSource src{B.seg_list + beg, B.seg_list2 + beg, cls < 0 ? 0 : B.seg_off[seg_id + 1] - beg, 0, cls, -1};
 
     // The first two couples, picked by lane 0 and shared with the segment.
     int a0 = -1, b0 = -1, a1 = -1, b1 = -1;
@@ -727,8 +737,8 @@ __device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int cls, 
         if ((it & 3) == 0 && !__any_sync(FULL_MASK, live)) break;
         const bool act = live && blk >= 0;
         const int c = blk * 4;
-        const int upa = __shfl_up_sync(FULL_MASK, nxa, 1, SEG); // lane l - 1's next couple
-        const int upb = __shfl_up_sync(FULL_MASK, nxb, 1, SEG);
+        const int upa = __shfl_up_sync(FULL_MASK, nxa, 1); // lane l - 1's next couple
+        const int upb = __shfl_up_sync(FULL_MASK, nxb, 1);
 
         // Blocks where both pairs have all 4 columns (and b is word-aligned)
         // take the short forms below; the pair edges take the checked ones.
@@ -736,7 +746,7 @@ __device__ __forceinline__ void stream_segment16(const BatchLaunch &B, int cls, 
 
         uint32_t vi[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1, SEG);
+        for (int j = 0; j < 4; ++j) vi[j] = __shfl_up_sync(FULL_MASK, vc[j], 1);
         if (sl == 0) {
             if (fast) {
 #pragma unroll
@@ -843,17 +853,26 @@ __global__ void __launch_bounds__(WARPS * 32, 16 / WARPS) comb_batch_kernel(cons
         const int code = B.class_code[cls];
 #define SLCS_CASE(TM, SEG)                                                                 \
     case TM * 100 + SEG:                                                                   \
-        stream_segment<TM, SEG, TNS>(B, cls, SEG_SLOTS * gw + lane / SEG, lane);                \
+        stream_segment<TM, SEG, TNS>(B, B.class_pool[cls], SEG_SLOTS * gw + lane / SEG, lane);  \
         break;
         switch (code) { SLCS_STREAM_CLASSES(SLCS_CASE) default: break; }
 #undef SLCS_CASE
         if (TNS == 4) {
+            if (code == PACKED16_VAR_CODE + VAR_TM * 100) {
+                // one call for every lane (idle lanes too), so that the warp
+                // runs a single copy of the body without diverging
+                const int e = B.lane_map[gw * 32 + lane];
+                const bool idle = e < 0;
+                stream_segment16<VAR_TM>(B, idle ? -1 : e >> 24, idle ? 0 : SEG_SLOTS * gw + ((e >> 16) & 0xff), lane,
+                                         idle ? 0 : (e >> 8) & 0xff, idle ? 1 : e & 0xff);
+            } else {
 #define SLCS_PCASE(TM, SEG)                                                                \
     case PACKED16_CODE + TM * 100 + SEG:                                                   \
-        stream_segment16<TM, SEG>(B, cls, SEG_SLOTS * gw + lane / SEG, lane);                   \
+        stream_segment16<TM>(B, B.class_pool[cls], SEG_SLOTS * gw + lane / SEG, lane, lane & (SEG - 1), SEG); \
         break;
-            switch (code) { SLCS_PACKED_CLASSES(SLCS_PCASE) default: break; }
+                switch (code) { SLCS_PACKED_CLASSES(SLCS_PCASE) default: break; }
 #undef SLCS_PCASE
+            }
         }
     }
     // Phase 2: stripes of pairs too tall to stream, whole warps, wavefront

@@ -43,7 +43,8 @@ inline int32_t pick_tw(int tm, int64_t chain, int64_t width, const void *b)
 // streamed: a segment of `seg` lanes combs pair after pair without draining
 // its pipeline between them.
 constexpr int MAX_CLASSES = 12;
-constexpr int SEG_SLOTS = 4; // segment slots per warp (32 / smallest SEG)
+constexpr int MAX_POOLS = 48; // item classes with a pool: fixed classes and the lane counts of the variable one
+constexpr int SEG_SLOTS = 8;  // segment slots per warp (32 / fewest lanes of a segment)
 struct BatchLaunch {
     CombLaunch wf;           // wavefront part (tasks of pairs too tall to stream)
     const int32_t *seg_off;  // device: SEG_SLOTS*nwarps+1 offsets into seg_list (CSR)
@@ -53,17 +54,28 @@ struct BatchLaunch {
     int32_t grid;            // blocks of the persistent launch
     int32_t nclass;          // stream classes; warp w serves the first class c with w < class_warp_end[c]
     int32_t class_warp_end[MAX_CLASSES];
-    int32_t class_code[MAX_CLASSES]; // rows per lane * 100 + lanes per segment (+ PACKED16_CODE when packed)
+    int32_t class_code[MAX_CLASSES]; // rows per lane * 100 + lanes per segment (+ PACKED16_CODE when packed;
+                                     // PACKED16_VAR_CODE + rows per lane for the variable class)
+    int32_t class_pool[MAX_CLASSES]; // the pool of a fixed class
+    // Variable class (its warps come first): per warp and lane, -1 (idle) or
+    // pool << 24 | segment slot << 16 | lane in the segment << 8 | lanes of the segment.
+    const int32_t *lane_map;
     // Pool of each class: items no segment list holds, claimed one at a time
     // (pool_ticket[c]) by segments of class c whose own lists are done.
     const int32_t *pool_list;        // device: pairs (packed classes: the low-half pair)
     const int32_t *pool_list2;       // device: packed classes: the high-half pair (-1: none)
-    int32_t *pool_ticket;            // device: MAX_CLASSES counters, zero at launch
-    int32_t pool_off[MAX_CLASSES + 1]; // CSR offsets of the classes' pools
+    int32_t *pool_ticket;            // device: MAX_POOLS counters, zero at launch
+    int32_t pool_off[MAX_POOLS + 1]; // CSR offsets of the pools
 };
 // Class-code offset of the packed variant: two pairs per register, strand ids
 // in 15 bits (pairs with m + n <= PACKED16_MAX_IDS), 4 columns per step.
 constexpr int PACKED16_CODE = 10000;
+// The variable packed class: segments of any lane count (4..32) side by side
+// in a warp, 16 rows per lane, so that a pair's rows are padded to a multiple
+// of 16 instead of to a class height.
+constexpr int PACKED16_VAR_CODE = 20000;
+constexpr int VAR_TM = 16;
+constexpr int VAR_MIN_LANES = 4;
 constexpr int PACKED16_MAX_IDS = 32767;
 bool packed16_supported(int tm, int seg);
 
