@@ -681,7 +681,7 @@ slcs_status slcs_comb_pair_words_host(const int32_t *a, int32_t m, const int32_t
 }
 
 static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_desc *pairs, int32_t npairs,
-                                    const slcs_config *cfg);
+                                    const slcs_config *cfg, bool var_class = true);
 static void plan_add_chunks(slcs_batch_plan *P, const slcs_pair_desc *pairs, int32_t npairs, const slcs_config *cfg);
 
 slcs_status slcs_batch_plan_create(slcs_batch_plan **plan_out, const slcs_pair_desc *pairs, int32_t npairs,
@@ -731,7 +731,7 @@ static void plan_add_chunks(slcs_batch_plan *P, const slcs_pair_desc *pairs, int
             k.o_hi = std::max(k.o_hi, d.out_offset + d.m + d.n);
         }
         // Sub-plan over the chunk's pairs (offsets stay global).
-        if (plan_create_impl(&k.plan, pairs + p0, p1 - p0, cfg) != SLCS_OK) {
+        if (plan_create_impl(&k.plan, pairs + p0, p1 - p0, cfg, false) != SLCS_OK) {
             for (auto &x : ch) slcs_batch_plan_destroy(x.plan);
             if (k.plan) slcs_batch_plan_destroy(k.plan);
             return;
@@ -773,7 +773,7 @@ static void plan_add_chunks(slcs_batch_plan *P, const slcs_pair_desc *pairs, int
 }
 
 static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_desc *pairs, int32_t npairs,
-                                    const slcs_config *cfg)
+                                    const slcs_config *cfg, bool var_class)
 {
     if (!plan_out) return fail(SLCS_ERR_INVALID, "plan is null");
     *plan_out = nullptr;
@@ -840,8 +840,13 @@ static slcs_status plan_create_impl(slcs_batch_plan **plan_out, const slcs_pair_
             // (16 rows per lane, segments of VAR_MIN_LANES..32 lanes side by
             // side in a warp), so that a pair's rows are padded to a multiple
             // of 16 rather than to one of a few class heights.
-            if (pack)
+            // (The sub-plans of a chunked host run keep the fixed packed
+            // classes at 8 warps per SM: their chunks of ~1,700 pairs measured
+            // 0.584 ms per host run that way, 0.656 ms with the variable class.)
+            if (pack && var_class)
                 for (int l = VAR_MIN_LANES; l <= 32; ++l) P->classes.push_back({VAR_TM, l, true, true});
+            else if (pack)
+                for (int t : {4, 8, 12, 16}) P->classes.push_back({t, 16, true});
             for (int t : {4, 8, 12, 16}) P->classes.push_back({t, 16, false});
             P->classes.push_back({12, 32, false});
             P->classes.push_back({16, 32, false});
